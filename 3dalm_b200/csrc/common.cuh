@@ -1,0 +1,216 @@
+// Shared device-side definitions: field layout in HBM, launch geometry,
+// deterministic grid reductions.
+//
+// Layout.  Every field is SoA (one array per component) over the stored grid
+// (interior + gc guide cells per side).  k (z) is contiguous like the
+// reference (src/util.h:11-13), but each k-row is padded to a pitch that is
+// a multiple of 8 elements and shifted by `off` so that the first interior
+// cell k = gc of every row starts on a 64-byte (FP64) / 32-byte (FP32)
+// boundary: a warp reading 32 consecutive interior cells touches exactly
+// 8 (FP64) or 4 (FP32) 32-byte sectors.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include <cuda_runtime.h>
+
+namespace dalm {
+
+#define DALM_CUDA(call)                                                              \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess)                                                       \
+            throw ::dalm::CudaError(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string &m) : std::runtime_error(m) {}
+};
+
+struct Grid {
+    int nx, ny, nz, gc;      // stored sizes (incl. guide cells) and guide cells
+    long long sx, sy, off;   // element strides and row offset
+    long long total;         // elements per field allocation
+
+    __host__ __device__ long long at(int i, int j, int k) const {
+        return (long long)i * sx + (long long)j * sy + k + off;
+    }
+    static Grid make(int nx, int ny, int nz, int gc) {
+        Grid g;
+        g.nx = nx; g.ny = ny; g.nz = nz; g.gc = gc;
+        g.off = (8 - gc % 8) % 8;
+        g.sy = ((g.off + nz + 7) / 8) * 8;
+        g.sx = g.sy * ny;
+        g.total = g.sx * nx;
+        return g;
+    }
+    // interior extents
+    __host__ __device__ int ni() const { return nx - 2 * gc; }
+    __host__ __device__ int nj() const { return ny - 2 * gc; }
+    __host__ __device__ int nk() const { return nz - 2 * gc; }
+};
+
+// A box of cells [lo, hi) per axis in stored indices.
+struct Box {
+    int lo[3], hi[3];
+    __host__ __device__ bool empty() const {
+        return hi[0] <= lo[0] || hi[1] <= lo[1] || hi[2] <= lo[2];
+    }
+    __host__ __device__ bool contains(int i, int j, int k) const {
+        return i >= lo[0] && i < hi[0] && j >= lo[1] && j < hi[1] && k >= lo[2] && k < hi[2];
+    }
+};
+
+// Tiling of a box into (32 k) x (8 j) x (1 i) tiles; blocks of 256 threads
+// walk the tiles with a block-stride loop so the number of blocks (and thus
+// the number of reduction partials) is fixed per launch.
+constexpr int TK = 32, TJ = 8, TILE_THREADS = TK * TJ;
+
+struct Tiling {
+    Box box;
+    int ntk, ntj, nti;
+    long long ntiles;
+    __host__ static Tiling make(const Box &b) {
+        Tiling t;
+        t.box = b;
+        t.ntk = (b.hi[2] - b.lo[2] + TK - 1) / TK;
+        t.ntj = (b.hi[1] - b.lo[1] + TJ - 1) / TJ;
+        t.nti = b.hi[0] - b.lo[0];
+        if (b.empty()) t.ntk = t.ntj = t.nti = 0;
+        t.ntiles = (long long)t.ntk * t.ntj * t.nti;
+        return t;
+    }
+    // cell handled by this thread in tile `tile`; false when outside the box
+    __device__ bool cell(long long tile, int &i, int &j, int &k) const {
+        int tk = (int)(tile % ntk);
+        long long r = tile / ntk;
+        int tj = (int)(r % ntj);
+        int ti = (int)(r / ntj);
+        k = box.lo[2] + tk * TK + (int)(threadIdx.x % TK);
+        j = box.lo[1] + tj * TJ + (int)(threadIdx.x / TK);
+        i = box.lo[0] + ti;
+        return k < box.hi[2] && j < box.hi[1];
+    }
+};
+
+// ---- deterministic reductions ---------------------------------------------
+//
+// Each block reduces its values in a fixed order (warp shuffles, then warps
+// in order) and writes one partial per block.  The last block to finish
+// (atomic ticket) sums the partials in block order and runs the finisher.
+// The result is independent of block scheduling; no block ever waits on
+// another, so there is no spin-wait anywhere.
+
+template <int N>
+struct Partials {
+    double *buf;            // [max_blocks][N]
+    unsigned int *ticket;   // one counter, reset by the last block
+};
+
+// Slot m of a reduction is a max when bit m of `maxmask` is set, else a sum.
+__device__ inline double red_op(double a, double b, bool is_max) {
+    return is_max ? (a > b ? a : b) : a + b;
+}
+
+__device__ inline double warp_reduce(double v, bool is_max) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = red_op(v, __shfl_down_sync(0xffffffffu, v, o), is_max);
+    return v;
+}
+
+// Block reduction of N values; result valid in thread 0.
+template <int N>
+__device__ inline void block_reduce(double (&v)[N], unsigned maxmask, double *smem /*[32*N]*/) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int m = 0; m < N; m++) v[m] = warp_reduce(v[m], (maxmask >> m) & 1u);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int m = 0; m < N; m++) smem[warp * N + m] = v[m];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+            double a = smem[m];
+            for (int w = 1; w < nwarps; w++) a = red_op(a, smem[w * N + m], (maxmask >> m) & 1u);
+            v[m] = a;
+        }
+    }
+    __syncthreads();
+}
+
+// Writes this block's partials; returns true in every thread of the last
+// block, whose thread 0 then holds the grid totals in v.  Max slots assume
+// non-negative values (identity 0).
+template <int N>
+__device__ inline bool grid_reduce(double (&v)[N], unsigned maxmask, Partials<N> P) {
+    __shared__ double smem[32 * N];
+    __shared__ bool is_last;
+    block_reduce<N>(v, maxmask, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int m = 0; m < N; m++) P.buf[blockIdx.x * N + m] = v[m];
+        __threadfence();
+        unsigned int t = atomicAdd(P.ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    // last block: fixed-order sum of the partials (each thread a fixed
+    // strided subset in block order, then the block reduction in warp order)
+    double acc[N];
+#pragma unroll
+    for (int m = 0; m < N; m++) acc[m] = 0.0;
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int m = 0; m < N; m++) {
+            double x = ((volatile double *)P.buf)[b * N + m];
+            acc[m] = (b == threadIdx.x) ? x : red_op(acc[m], x, (maxmask >> m) & 1u);
+        }
+    }
+    block_reduce<N>(acc, maxmask, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int m = 0; m < N; m++) v[m] = acc[m];
+        *P.ticket = 0u;
+    }
+    return true;
+}
+
+// Kinds of kernels, for launch counting and per-kernel event timing.
+enum KernelKind {
+    KK_PREDICT = 0, KK_FLUX_RHS, KK_PBC, KK_PROJECT, KK_UBC, KK_DIAG, KK_TAVG,
+    KK_ALM_POINTS, KK_ALM_SUMS, KK_ALM_PROJECT,
+    KK_SOR_SWEEP, KK_RESIDUAL_NORM, KK_JACOBI_SWEEP,
+    KK_BICG_INIT, KK_BICG_P, KK_BICG_Q, KK_BICG_S, KK_BICG_T, KK_BICG_XR,
+    KK_POISSON_BEGIN, KK_LAYOUT, KK_COUNT
+};
+
+// Everything a launcher needs besides its operands: the stream, the number
+// of blocks for tile loops, and an optional hook called around each launch
+// (the host uses it to record CUDA events per kernel kind).
+struct LaunchCtx {
+    cudaStream_t s = 0;
+    int blocks = 1;
+    void (*hook)(void *self, int kind, int phase) = nullptr;  // phase 0 before, 1 after
+    void *self = nullptr;
+    long long *launches = nullptr;
+    void pre(int kind) const {
+        if (hook) hook(self, kind, 0);
+    }
+    void post(int kind) const {
+        if (launches) (*launches)++;
+        if (hook) hook(self, kind, 1);
+        DALM_CUDA(cudaGetLastError());
+    }
+};
+
+inline int reduction_blocks(int sm_count) { return sm_count * 8; }
+
+}  // namespace dalm

@@ -1,0 +1,922 @@
+// C ABI (include/dalm.h) and the host orchestration of one time step.
+//
+// The handle owns all device state of one case on one GPU and one stream.
+// A step enqueues the stage kernels in the order of Solver::main_loop_once
+// (src/solver.h:1034-1306); the only host synchronisation inside a step is
+// the Poisson loop's convergence poll, once per batch of iterations.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dalm.h"
+#include "alm.cuh"
+#include "case_io.hpp"
+#include "poisson.cuh"
+
+using namespace dalm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr double PI_D = 3.14159265358979323846;
+// Truncation radius of the Gaussian projection: r^2 <= 40 eps^2, where the
+// dropped weight exp(-40) ~ 4e-18 of the peak is below FP64 resolution of f.
+constexpr double ALM_CUTOFF_EPS2 = 40.0;
+
+const char *kKindNames[KK_COUNT] = {
+    "predict", "flux_rhs", "pressure_bc", "project", "velocity_bc", "diag", "tavg",
+    "alm_points", "alm_sums", "alm_project",
+    "sor_sweep", "residual_norm", "jacobi_sweep",
+    "bicg_init", "bicg_p", "bicg_q", "bicg_s", "bicg_t", "bicg_xr",
+    "poisson_begin", "layout"};
+
+struct EventPair {
+    cudaEvent_t a, b;
+    int kind;
+};
+
+}  // namespace
+
+struct dalm_handle {
+    CaseData cs;
+    dalm_options opt;
+    Grid g;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    LaunchCtx L;
+    std::string err;
+    std::vector<void *> allocs;
+
+    // mesh and coefficients
+    MeshDev mesh{};
+    PoissonCoef coef{};
+    StepParams P{};
+    // fields
+    double *U[2][3] = {};
+    int ucur = 0;
+    double *JU[2][3] = {};
+    int jcur = 0;
+    double *F[3] = {};
+    double *Pp = nullptr, *B = nullptr;
+    double *Utavg[3] = {};
+    double *scratch = nullptr;   // one scalar field for nut / div output
+    double *staging = nullptr;   // reference-layout staging buffer (3*len)
+    PoissonBufs pb{};
+    PoissonConfig pcfg{};
+    double *partial = nullptr;
+    unsigned int *ticket = nullptr;
+    KrylovState *d_kst = nullptr, *h_kst = nullptr;
+    DiagState *d_diag = nullptr, *h_diag = nullptr;
+    double *d_prof = nullptr;
+    // actuator line
+    AlmDev alm{};
+    std::vector<TurbineDev> h_wt;
+    std::vector<double> base_twist, twist;
+    double *h_wt_out = nullptr;  // pinned: torque[T], thrust[T]
+    Box fbox{{0, 0, 0}, {0, 0, 0}};
+    // runtime
+    int64_t step = 0, tavg_count = 0, last_it = 0;
+    int64_t max_it = 0;
+    double tol = 0;
+    long long launch_count = 0;
+    // profiling
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<EventPair> ev_pending;
+    cudaEvent_t ev_open = nullptr;
+    double kind_ms[KK_COUNT] = {};
+    int64_t kind_launches[KK_COUNT] = {};
+    double stage_ms[7] = {};
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_pending;
+
+    ~dalm_handle() { release(); }
+
+    void release() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : allocs) cudaFree(p);
+        allocs.clear();
+        if (h_kst) cudaFreeHost(h_kst);
+        if (h_diag) cudaFreeHost(h_diag);
+        if (h_wt_out) cudaFreeHost(h_wt_out);
+        h_kst = nullptr; h_diag = nullptr; h_wt_out = nullptr;
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        for (auto &p : ev_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+        for (auto &p : stage_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+        ev_pool.clear(); ev_pending.clear(); stage_pending.clear();
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+
+    template <typename T>
+    T *dalloc(size_t n) {
+        void *p = nullptr;
+        DALM_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+        DALM_CUDA(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+        allocs.push_back(p);
+        return (T *)p;
+    }
+    template <typename T>
+    T *upload(const std::vector<T> &v) {
+        T *p = dalloc<T>(v.size());
+        if (!v.empty())
+            DALM_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return p;
+    }
+
+    // ---- profiling -------------------------------------------------------
+    cudaEvent_t take_event() {
+        if (ev_pool.empty()) {
+            cudaEvent_t e;
+            DALM_CUDA(cudaEventCreate(&e));
+            return e;
+        }
+        cudaEvent_t e = ev_pool.back();
+        ev_pool.pop_back();
+        return e;
+    }
+    static void hook(void *self, int kind, int phase) {
+        dalm_handle *h = (dalm_handle *)self;
+        cudaEvent_t e = h->take_event();
+        DALM_CUDA(cudaEventRecord(e, h->stream));
+        if (phase == 0) {
+            h->ev_open = e;
+        } else {
+            h->ev_pending.push_back({h->ev_open, e, kind});
+            h->ev_open = nullptr;
+        }
+    }
+    void harvest() {
+        for (auto &p : ev_pending) {
+            DALM_CUDA(cudaEventSynchronize(p.b));
+            float ms = 0;
+            DALM_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+            kind_ms[p.kind] += ms;
+            kind_launches[p.kind] += 1;
+            ev_pool.push_back(p.a);
+            ev_pool.push_back(p.b);
+        }
+        ev_pending.clear();
+        for (auto &p : stage_pending) {
+            DALM_CUDA(cudaEventSynchronize(p.second.second));
+            float ms = 0;
+            DALM_CUDA(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+            stage_ms[p.first] += ms;
+            ev_pool.push_back(p.second.first);
+            ev_pool.push_back(p.second.second);
+        }
+        stage_pending.clear();
+    }
+    struct StageTimer {
+        dalm_handle *h;
+        int stage;
+        cudaEvent_t a = nullptr;
+        StageTimer(dalm_handle *h_, int s) : h(h_), stage(s) {
+            if (h->opt.profile) {
+                a = h->take_event();
+                DALM_CUDA(cudaEventRecord(a, h->stream));
+            }
+        }
+        ~StageTimer() noexcept(false) {
+            if (a) {
+                cudaEvent_t b = h->take_event();
+                DALM_CUDA(cudaEventRecord(b, h->stream));
+                h->stage_pending.push_back({stage, {a, b}});
+            }
+        }
+    };
+
+    // ---- construction ----------------------------------------------------
+    void init(const std::string &dir, const dalm_options &o) {
+        opt = o;
+        if (opt.precision != DALM_FP64)
+            throw std::invalid_argument("only DALM_FP64 precision is available in this build");
+        if (opt.limiter != DALM_LIMITER_MINMOD)
+            throw std::invalid_argument("only the minmod limiter is available in this build");
+        cs = load_case(dir);
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            throw CudaError("no CUDA device is available");
+        if (opt.device < 0 || opt.device >= ndev) throw std::invalid_argument("bad device ordinal");
+        DALM_CUDA(cudaSetDevice(opt.device));
+        DALM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, opt.device));
+        DALM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        g = Grid::make((int)cs.size[0], (int)cs.size[1], (int)cs.size[2], (int)cs.gc);
+        L.s = stream;
+        L.blocks = reduction_blocks(sm_count);
+        L.launches = &launch_count;
+        if (opt.profile) {
+            L.hook = &dalm_handle::hook;
+            L.self = this;
+        }
+        max_it = cs.max_it;
+        tol = cs.tol;
+
+        // mesh
+        mesh.x = upload(cs.x); mesh.y = upload(cs.y); mesh.z = upload(cs.z);
+        mesh.dx = upload(cs.dx); mesh.dy = upload(cs.dy); mesh.dz = upload(cs.dz);
+        build_coefficients();
+
+        size_t n = (size_t)g.total;
+        for (int b = 0; b < 2; b++)
+            for (int m = 0; m < 3; m++) {
+                U[b][m] = dalloc<double>(n);
+                JU[b][m] = dalloc<double>(n);
+            }
+        for (int m = 0; m < 3; m++) {
+            F[m] = dalloc<double>(n);
+            Utavg[m] = dalloc<double>(n);
+        }
+        Pp = dalloc<double>(n);
+        B = dalloc<double>(n);
+        double **kv[] = {&pb.r, &pb.r0, &pb.pk, &pb.q, &pb.s, &pb.t, &pb.pp, &pb.ss, &pb.tp, &pb.ts};
+        for (auto v : kv) *v = dalloc<double>(n);
+        pb.x = Pp;
+        pb.b = B;
+        pcfg.method = cs.method == "BiCG" ? PM_BICG : (cs.method == "SOR" ? PM_SOR : PM_JACOBI);
+        pcfg.pc = cs.pc_method == "SOR" ? PC_SOR : PC_JACOBI;
+        pcfg.relax = cs.relax;
+        pcfg.pc_relax = cs.pc_relax;
+        pcfg.pc_sweeps = (int)cs.pc_max_it;
+        partial = dalloc<double>((size_t)L.blocks * 4);
+        ticket = dalloc<unsigned int>(1);
+        d_kst = dalloc<KrylovState>(1);
+        d_diag = dalloc<DiagState>(1);
+        DALM_CUDA(cudaHostAlloc((void **)&h_kst, sizeof(KrylovState), cudaHostAllocDefault));
+        DALM_CUDA(cudaHostAlloc((void **)&h_diag, sizeof(DiagState), cudaHostAllocDefault));
+        memset(h_kst, 0, sizeof(KrylovState));
+        memset(h_diag, 0, sizeof(DiagState));
+        DiagState d0{};
+        d0.ncell = (double)g.ni() * g.nj() * g.nk();
+        DALM_CUDA(cudaMemcpy(d_diag, &d0, sizeof(d0), cudaMemcpyHostToDevice));
+
+        P.g = g;
+        P.m = mesh;
+        P.re = cs.re; P.cs = cs.cs; P.dt = cs.dt; P.max_diag = cs.max_diag;
+        for (int m = 0; m < 3; m++) P.uin[m] = cs.uin[m];
+        P.prof = nullptr;
+        P.fbox = fbox;
+
+        init_alm();
+
+        // Solver::initialize tail (src/solver.h:737-833): U = Uold = Uin,
+        // p = 0, BCs, flux, nut/div (on demand here), ALM force, diagnostics.
+        for (int b = 0; b < 2; b++)
+            for (int m = 0; m < 3; m++) launch_fill(L, U[b][m], g.total, cs.uin[m]);
+        refresh_after_state(DALM_SET_APPLY_UBC | DALM_SET_RECOMPUTE_JU, nullptr);
+        DALM_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // build_A (src/eq.h:701-798) as per-axis arrays; see PoissonCoef.
+    void build_coefficients() {
+        int64_t gc = cs.gc, NX = cs.size[0], NY = cs.size[1], NZ = cs.size[2];
+        double md = cs.max_diag;
+        std::vector<double> ex(NX, 0), awu(NX, 0), ae(NX, 0), aw(NX, 0);
+        std::vector<double> anu(NY, 0), asu(NY, 0), an(NY, 0), as(NY, 0);
+        std::vector<double> atu(NZ, 0), abu(NZ, 0), at(NZ, 0), ab(NZ, 0);
+        for (int64_t i = gc; i < NX - gc; i++) {
+            if (i < NX - gc - 1) {
+                double v = 1 / (cs.dx[i] * (cs.x[i + 1] - cs.x[i]));
+                ex[i] = v;
+                ae[i] = v / md;
+            } else {
+                ex[i] = 2 / (cs.dx[i] * cs.dx[i]);
+            }
+            if (i > gc) {
+                awu[i] = 1 / (cs.dx[i] * (cs.x[i] - cs.x[i - 1]));
+                aw[i] = awu[i] / md;
+            }
+        }
+        for (int64_t j = gc; j < NY - gc; j++) {
+            if (j < NY - gc - 1) { anu[j] = 1 / (cs.dy[j] * (cs.y[j + 1] - cs.y[j])); an[j] = anu[j] / md; }
+            if (j > gc) { asu[j] = 1 / (cs.dy[j] * (cs.y[j] - cs.y[j - 1])); as[j] = asu[j] / md; }
+        }
+        for (int64_t k = gc; k < NZ - gc; k++) {
+            if (k < NZ - gc - 1) { atu[k] = 1 / (cs.dz[k] * (cs.z[k + 1] - cs.z[k])); at[k] = atu[k] / md; }
+            if (k > gc) { abu[k] = 1 / (cs.dz[k] * (cs.z[k] - cs.z[k - 1])); ab[k] = abu[k] / md; }
+        }
+        coef.ex = upload(ex); coef.aw_u = upload(awu);
+        coef.an_u = upload(anu); coef.as_u = upload(asu);
+        coef.at_u = upload(atu); coef.ab_u = upload(abu);
+        coef.ae = upload(ae); coef.aw = upload(aw);
+        coef.an = upload(an); coef.as = upload(as);
+        coef.at = upload(at); coef.ab = upload(ab);
+        coef.max_diag = md;
+    }
+
+    void init_alm() {
+        int64_t T = (int64_t)cs.turbines.size();
+        alm.wt_count = (int)T;
+        alm.ap_count = (int)cs.ap_count();
+        if (alm.ap_count == 0) return;
+        alm.ap_per_blade = (int)cs.ap_per_blade;
+        alm.blades = (int)cs.blades;
+        alm.ap_per_wt = (int)(cs.blades * cs.ap_per_blade);
+        alm.atk_count = (int)cs.atk_count;
+        double pw = cs.projection_width;
+        alm.pw2 = pw * pw;
+        double c = pw * sqrt(PI_D);
+        alm.e_coef = 1 / (c * c * c);  // 1/cubic(pw*sqrt(Pi)), src/alm.h:433
+        alm.cutoff2 = ALM_CUTOFF_EPS2 * alm.pw2;
+        for (auto &t : cs.turbines) {
+            TurbineDev d{};
+            for (int m = 0; m < 3; m++) { d.base[m] = t.base[m]; d.rot_center[m] = t.rot_center[m]; }
+            for (int m = 0; m < 4; m++) d.formula[m] = t.formula[m];
+            d.rot_speed = t.rot_speed;
+            d.type = t.angle_type;
+            h_wt.push_back(d);
+        }
+        base_twist = cs.ap_twist;
+        twist = cs.ap_twist;
+        alm.wt = upload(h_wt);
+        alm.r = upload(cs.ap_r);
+        alm.dr = upload(cs.ap_dr);
+        alm.chord = upload(cs.ap_chord);
+        alm.twist = upload(twist);
+        alm.cd = upload(cs.ap_cd);
+        alm.cl = upload(cs.ap_cl);
+        alm.atk = upload(cs.atk);
+        alm.pt_xyz = dalloc<double>(3 * alm.ap_count);
+        alm.pt_f = dalloc<double>(3 * alm.ap_count);
+        alm.pt_torque = dalloc<double>(alm.ap_count);
+        alm.pt_thrust = dalloc<double>(alm.ap_count);
+        alm.wt_torque = dalloc<double>(T);
+        alm.wt_thrust = dalloc<double>(T);
+        DALM_CUDA(cudaHostAlloc((void **)&h_wt_out, sizeof(double) * 2 * T, cudaHostAllocDefault));
+        memset(h_wt_out, 0, sizeof(double) * 2 * T);
+    }
+
+    // ---- views -----------------------------------------------------------
+    Vec3<double> u_cur() { return {{U[ucur][0], U[ucur][1], U[ucur][2]}}; }
+    Vec3<double> u_old() { return {{U[1 - ucur][0], U[1 - ucur][1], U[1 - ucur][2]}}; }
+    Vec3<double> ju_cur() { return {{JU[jcur][0], JU[jcur][1], JU[jcur][2]}}; }
+    Vec3<double> ju_other() { return {{JU[1 - jcur][0], JU[1 - jcur][1], JU[1 - jcur][2]}}; }
+    static Vec3<const double> c(Vec3<double> v) { return {{v.c[0], v.c[1], v.c[2]}}; }
+    Vec3<double> f3() { return {{F[0], F[1], F[2]}}; }
+
+    // ---- stages ----------------------------------------------------------
+    void stage_predict() {
+        StageTimer t(this, DALM_STAGE_PREDICT);
+        P.fbox = fbox;
+        launch_predict(L, P, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
+        ucur = 1 - ucur;  // the old buffer is now Uold
+    }
+    void stage_flux_rhs() {
+        StageTimer t(this, DALM_STAGE_FLUX_RHS);
+        launch_flux_rhs(L, P, c(u_cur()), ju_cur(), B);
+    }
+    void enqueue_poisson_iteration() {
+        if (pcfg.method == PM_BICG) {
+            launch_bicg_iteration(L, g, coef, pb, pcfg, Partials<2>{partial, ticket}, d_kst);
+        } else if (pcfg.method == PM_SOR) {
+            launch_sor_iteration(L, g, coef, pb, pcfg.relax, Partials<1>{partial, ticket}, d_kst);
+        } else {
+            launch_jacobi_iteration(L, g, coef, pb, Partials<1>{partial, ticket}, d_kst);
+        }
+    }
+    void stage_poisson() {
+        StageTimer t(this, DALM_STAGE_POISSON);
+        double ncell = (double)g.ni() * g.nj() * g.nk();
+        launch_poisson_begin(L, d_kst, max_it, tol, ncell);
+        if (pcfg.method == PM_BICG) launch_bicg_init(L, g, coef, pb, Partials<1>{partial, ticket}, d_kst);
+        long long issued = 0;
+        long long batch = opt.poisson_batch > 0 ? opt.poisson_batch
+                                                : std::max<long long>(4, last_it > 0 ? last_it : 16);
+        while (true) {
+            for (long long n = 0; n < batch; n++) enqueue_poisson_iteration();
+            issued += batch;
+            DALM_CUDA(cudaMemcpyAsync(h_kst, d_kst, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream));
+            DALM_CUDA(cudaStreamSynchronize(stream));
+            if (h_kst->done) break;
+            if (issued > max_it + 1)
+                throw std::runtime_error("Poisson loop did not stop at its iteration limit");
+            batch = opt.poisson_batch > 0 ? opt.poisson_batch
+                                          : std::max<long long>(4, std::min<long long>(64, issued / 8));
+        }
+        last_it = h_kst->it;
+    }
+    void stage_project() {
+        StageTimer t(this, DALM_STAGE_PROJECT);
+        launch_pressure_bc(L, P, Pp);
+        launch_project(L, P, u_cur(), ju_cur(), ju_other(), Pp, Partials<2>{partial, ticket}, d_diag);
+        jcur = 1 - jcur;
+        launch_velocity_bc(L, P, u_cur(), c(u_old()));
+        DALM_CUDA(cudaMemcpyAsync(h_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToHost, stream));
+    }
+
+    // Blade-point positions on the host (same formulas as the device) to
+    // bound the cells the truncated Gaussians can reach.
+    Box force_box(double tm) {
+        Box b{{0, 0, 0}, {0, 0, 0}};
+        if (alm.ap_count == 0) return b;
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int a = 0; a < alm.ap_count; a++) {
+            const TurbineDev &wt = h_wt[a / alm.ap_per_wt];
+            double angle = wt.formula[0] * sin(wt.formula[1] * tm + wt.formula[2]) + wt.formula[3];
+            int bid = (a % alm.ap_per_wt) / alm.ap_per_blade;
+            double r = cs.ap_r[a];
+            double th = bid * (2 * PI_D / alm.blades) + tm * wt.rot_speed;
+            double in[3] = {wt.rot_center[0], wt.rot_center[1] + r * cos(th), wt.rot_center[2] + r * sin(th)};
+            double cc = cos(-angle), ss = sin(-angle), out[3];
+            switch (wt.type) {
+            case EULER_ROLL: out[0] = in[0]; out[1] = cc * in[1] + ss * in[2]; out[2] = -ss * in[1] + cc * in[2]; break;
+            case EULER_PITCH: out[0] = cc * in[0] - ss * in[2]; out[1] = in[1]; out[2] = -ss * in[0] + cc * in[2]; break;
+            case EULER_YAW: out[0] = cc * in[0] + ss * in[1]; out[1] = -ss * in[0] + cc * in[1]; out[2] = in[2]; break;
+            default: out[0] = in[0]; out[1] = in[1]; out[2] = in[2]; break;
+            }
+            for (int m = 0; m < 3; m++) {
+                double v = out[m] + wt.base[m];
+                lo[m] = std::min(lo[m], v);
+                hi[m] = std::max(hi[m], v);
+            }
+        }
+        double R = sqrt(alm.cutoff2);
+        const std::vector<double> *ax[3] = {&cs.x, &cs.y, &cs.z};
+        for (int m = 0; m < 3; m++) {
+            const std::vector<double> &c = *ax[m];
+            int n = (int)c.size(), gc = (int)cs.gc;
+            int l = (int)(std::lower_bound(c.begin(), c.end(), lo[m] - R) - c.begin()) - 1;
+            int h = (int)(std::upper_bound(c.begin(), c.end(), hi[m] + R) - c.begin()) + 1;
+            b.lo[m] = std::max(gc, l);
+            b.hi[m] = std::min(n - gc, h);
+        }
+        if (b.empty()) b = Box{{0, 0, 0}, {0, 0, 0}};
+        return b;
+    }
+
+    static Box unite(const Box &a, const Box &b) {
+        if (a.empty()) return b;
+        if (b.empty()) return a;
+        Box u;
+        for (int m = 0; m < 3; m++) {
+            u.lo[m] = std::min(a.lo[m], b.lo[m]);
+            u.hi[m] = std::max(a.hi[m], b.hi[m]);
+        }
+        return u;
+    }
+
+    void stage_alm() {
+        if (alm.ap_count == 0) return;
+        StageTimer t(this, DALM_STAGE_ALM);
+        double tm = cs.dt * (double)step;  // rt.get_time(), src/solver.h:189-191
+        launch_alm_points(L, P, alm, tm, c(u_cur()));
+        Box cur = force_box(tm);
+        launch_alm_project(L, P, alm, unite(fbox, cur), f3());
+        fbox = cur;
+        DALM_CUDA(cudaMemcpyAsync(h_wt_out, alm.wt_torque, sizeof(double) * alm.wt_count,
+                                  cudaMemcpyDeviceToHost, stream));
+        DALM_CUDA(cudaMemcpyAsync(h_wt_out + alm.wt_count, alm.wt_thrust, sizeof(double) * alm.wt_count,
+                                  cudaMemcpyDeviceToHost, stream));
+    }
+    void stage_diag() {
+        StageTimer t(this, DALM_STAGE_DIAG);
+        launch_diag(L, P, c(u_cur()), c(ju_cur()), Partials<2>{partial, ticket}, d_diag);
+        DALM_CUDA(cudaMemcpyAsync(h_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToHost, stream));
+    }
+    void stage_tavg() {
+        if (!opt.time_average) return;
+        double tm = cs.dt * (double)step;
+        if (!(tm >= cs.tavg_start_time)) return;
+        StageTimer t(this, DALM_STAGE_TAVG);
+        tavg_count++;
+        double w = 1. / tavg_count;
+        launch_tavg(L, g, {{Utavg[0], Utavg[1], Utavg[2]}}, c(u_cur()), w);
+    }
+
+    void run_stage(int s) {
+        switch (s) {
+        case DALM_STAGE_PREDICT: stage_predict(); break;
+        case DALM_STAGE_FLUX_RHS: stage_flux_rhs(); break;
+        case DALM_STAGE_POISSON: stage_poisson(); break;
+        case DALM_STAGE_PROJECT: stage_project(); break;
+        case DALM_STAGE_ALM: stage_alm(); break;
+        case DALM_STAGE_DIAG: stage_diag(); break;
+        case DALM_STAGE_TAVG: stage_tavg(); break;
+        default: throw std::invalid_argument("unknown stage");
+        }
+    }
+
+    // Solver::main_loop_once (src/solver.h:1034-1306)
+    void step_once() {
+        if (step != 0) {
+            stage_predict();
+            stage_flux_rhs();
+            stage_poisson();
+            stage_project();
+            stage_alm();
+        }
+        stage_tavg();
+        step++;
+    }
+
+    // derived quantities after a state change (src/solver.h:767-833)
+    void refresh_after_state(int flags, const double *JU_host) {
+        if (flags & DALM_SET_APPLY_UBC) {
+            for (int m = 0; m < 3; m++)
+                DALM_CUDA(cudaMemcpyAsync(U[1 - ucur][m], U[ucur][m], sizeof(double) * g.total,
+                                          cudaMemcpyDeviceToDevice, stream));
+            launch_velocity_bc(L, P, u_cur(), c(u_old()));
+        }
+        if ((flags & DALM_SET_RECOMPUTE_JU) || !JU_host) {
+            launch_flux_only(L, P, c(u_cur()), ju_cur());
+        } else {
+            upload_field(JU_host, 3, JU[jcur]);
+            upload_field(JU_host, 3, JU[1 - jcur]);
+        }
+        stage_alm();
+        stage_diag();
+    }
+
+    // ---- host <-> device layout -----------------------------------------
+    double *stage_buffer() {
+        if (!staging) staging = dalloc<double>((size_t)3 * g.nx * g.ny * g.nz);
+        return staging;
+    }
+    void upload_field(const double *host, int nc, double *const *dst) {
+        double *s = stage_buffer();
+        size_t bytes = sizeof(double) * (size_t)nc * g.nx * g.ny * g.nz;
+        DALM_CUDA(cudaMemcpyAsync(s, host, bytes, cudaMemcpyHostToDevice, stream));
+        launch_to_device_layout(L, g, s, nc, dst);
+        DALM_CUDA(cudaStreamSynchronize(stream));
+    }
+    void download_field(double *const *src, int nc, double *host) {
+        double *s = stage_buffer();
+        size_t bytes = sizeof(double) * (size_t)nc * g.nx * g.ny * g.nz;
+        launch_to_ref_layout(L, g, src, nc, s);
+        DALM_CUDA(cudaMemcpyAsync(host, s, bytes, cudaMemcpyDeviceToHost, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+    }
+    double *scratch_field() {
+        if (!scratch) scratch = dalloc<double>((size_t)g.total);
+        DALM_CUDA(cudaMemsetAsync(scratch, 0, sizeof(double) * g.total, stream));
+        return scratch;
+    }
+
+    void get_field(int which, double *out) {
+        switch (which) {
+        case DALM_FIELD_U: download_field(U[ucur], 3, out); break;
+        case DALM_FIELD_UOLD: download_field(U[1 - ucur], 3, out); break;
+        case DALM_FIELD_JU: download_field(JU[jcur], 3, out); break;
+        case DALM_FIELD_P: download_field(&Pp, 1, out); break;
+        case DALM_FIELD_NUT: {
+            double *s = scratch_field();
+            launch_nut_field(L, P, c(u_cur()), s);
+            download_field(&s, 1, out);
+            break;
+        }
+        case DALM_FIELD_DIV: {
+            double *s = scratch_field();
+            launch_div_field(L, P, c(ju_cur()), s);
+            download_field(&s, 1, out);
+            break;
+        }
+        case DALM_FIELD_F: download_field(F, 3, out); break;
+        case DALM_FIELD_B: download_field(&B, 1, out); break;
+        case DALM_FIELD_UTAVG: download_field(Utavg, 3, out); break;
+        default: throw std::invalid_argument("unknown field");
+        }
+    }
+    void set_field(int which, const double *in) {
+        switch (which) {
+        case DALM_FIELD_U: upload_field(in, 3, U[ucur]); break;
+        case DALM_FIELD_UOLD: upload_field(in, 3, U[1 - ucur]); break;
+        case DALM_FIELD_JU: upload_field(in, 3, JU[jcur]); upload_field(in, 3, JU[1 - jcur]); break;
+        case DALM_FIELD_P: upload_field(in, 1, &Pp); break;
+        case DALM_FIELD_F:
+            upload_field(in, 3, F);
+            fbox = Box{{(int)cs.gc, (int)cs.gc, (int)cs.gc},
+                       {g.nx - (int)cs.gc, g.ny - (int)cs.gc, g.nz - (int)cs.gc}};
+            break;
+        case DALM_FIELD_B: upload_field(in, 1, &B); break;
+        case DALM_FIELD_UTAVG: upload_field(in, 3, Utavg); break;
+        default: throw std::invalid_argument("field is derived and cannot be set");
+        }
+    }
+
+    void sync_stats() {
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        if (opt.profile) harvest();
+    }
+};
+
+// ---------------------------------------------------------------- C ABI
+
+#define API_BEGIN(h)                                   \
+    if (!(h)) {                                        \
+        g_last_error = "null handle";                  \
+        return DALM_ERR_ARG;                           \
+    }                                                  \
+    try {
+#define API_END(h)                                     \
+    }                                                  \
+    catch (const CudaError &e) {                       \
+        (h)->err = e.what();                           \
+        return DALM_ERR_CUDA;                          \
+    }                                                  \
+    catch (const std::invalid_argument &e) {           \
+        (h)->err = e.what();                           \
+        return DALM_ERR_ARG;                           \
+    }                                                  \
+    catch (const std::exception &e) {                  \
+        (h)->err = e.what();                           \
+        return DALM_ERR_CASE;                          \
+    }                                                  \
+    return DALM_OK;
+
+extern "C" {
+
+void dalm_default_options(dalm_options *opt) {
+    if (!opt) return;
+    memset(opt, 0, sizeof(*opt));
+    opt->precision = DALM_FP64;
+    opt->limiter = DALM_LIMITER_MINMOD;
+    opt->device = 0;
+    opt->time_average = 1;
+    opt->check_finite = 1;
+    opt->poisson_batch = 0;
+    opt->use_graphs = 1;
+    opt->profile = 0;
+}
+
+int dalm_create(const char *case_dir, const dalm_options *opt, dalm_handle **out) {
+    if (!case_dir || !out) {
+        g_last_error = "null argument";
+        return DALM_ERR_ARG;
+    }
+    *out = nullptr;
+    dalm_options o;
+    if (opt) o = *opt;
+    else dalm_default_options(&o);
+    std::unique_ptr<dalm_handle> h(new dalm_handle());
+    try {
+        h->init(case_dir, o);
+    } catch (const CudaError &e) {
+        g_last_error = e.what();
+        return DALM_ERR_CUDA;
+    } catch (const std::invalid_argument &e) {
+        g_last_error = e.what();
+        return DALM_ERR_ARG;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return DALM_ERR_CASE;
+    }
+    *out = h.release();
+    return DALM_OK;
+}
+
+void dalm_destroy(dalm_handle *h) { delete h; }
+
+const char *dalm_last_error(const dalm_handle *h) {
+    return h ? h->err.c_str() : g_last_error.c_str();
+}
+
+int dalm_get_size(dalm_handle *h, int64_t size[3], int64_t *gc) {
+    API_BEGIN(h)
+    if (size)
+        for (int m = 0; m < 3; m++) size[m] = h->cs.size[m];
+    if (gc) *gc = h->cs.gc;
+    API_END(h)
+}
+
+int dalm_get_mesh(dalm_handle *h, double *x, double *y, double *z, double *dx, double *dy,
+                  double *dz) {
+    API_BEGIN(h)
+    auto cp = [](double *d, const std::vector<double> &v) {
+        if (d) memcpy(d, v.data(), v.size() * sizeof(double));
+    };
+    cp(x, h->cs.x); cp(y, h->cs.y); cp(z, h->cs.z);
+    cp(dx, h->cs.dx); cp(dy, h->cs.dy); cp(dz, h->cs.dz);
+    API_END(h)
+}
+
+int dalm_get_runtime(dalm_handle *h, double *dt, int64_t *max_step) {
+    API_BEGIN(h)
+    if (dt) *dt = h->cs.dt;
+    if (max_step) *max_step = h->cs.max_step;
+    API_END(h)
+}
+
+int dalm_get_max_diag(dalm_handle *h, double *md) {
+    API_BEGIN(h)
+    if (!md) throw std::invalid_argument("null pointer");
+    *md = h->cs.max_diag;
+    API_END(h)
+}
+
+int dalm_set_state(dalm_handle *h, const double *U, const double *JU, const double *p, int flags) {
+    API_BEGIN(h)
+    if (!U) throw std::invalid_argument("U must not be null");
+    h->upload_field(U, 3, h->U[h->ucur]);
+    if (p) h->upload_field(p, 1, &h->Pp);
+    h->refresh_after_state(flags, JU);
+    h->sync_stats();
+    API_END(h)
+}
+
+int dalm_get_field(dalm_handle *h, int field, double *out) {
+    API_BEGIN(h)
+    if (!out) throw std::invalid_argument("null output");
+    h->get_field(field, out);
+    API_END(h)
+}
+
+int dalm_set_field(dalm_handle *h, int field, const double *in) {
+    API_BEGIN(h)
+    if (!in) throw std::invalid_argument("null input");
+    h->set_field(field, in);
+    API_END(h)
+}
+
+int dalm_set_inflow_profile(dalm_handle *h, const double *prof) {
+    API_BEGIN(h)
+    DALM_CUDA(cudaStreamSynchronize(h->stream));
+    if (!prof) {
+        h->P.prof = nullptr;
+    } else {
+        if (!h->d_prof) h->d_prof = h->dalloc<double>((size_t)3 * h->g.ny * h->g.nz);
+        DALM_CUDA(cudaMemcpy(h->d_prof, prof, sizeof(double) * 3 * h->g.ny * h->g.nz,
+                             cudaMemcpyHostToDevice));
+        h->P.prof = h->d_prof;
+    }
+    API_END(h)
+}
+
+int dalm_set_turbine_params(dalm_handle *h, const double *yaw_deg, const double *pitch_deg,
+                            const double *omega) {
+    API_BEGIN(h)
+    if (h->alm.ap_count == 0) return DALM_OK;
+    DALM_CUDA(cudaStreamSynchronize(h->stream));
+    int T = h->alm.wt_count, per = h->alm.ap_per_wt;
+    for (int w = 0; w < T; w++) {
+        TurbineDev &d = h->h_wt[w];
+        if (yaw_deg) {
+            d.type = EULER_YAW;
+            d.formula[0] = d.formula[1] = d.formula[2] = 0;
+            d.formula[3] = yaw_deg[w] * PI_D / 180;  // deg_to_rad, src/util.h:214-216
+        }
+        if (omega) d.rot_speed = omega[w];
+        if (pitch_deg)
+            for (int a = w * per; a < (w + 1) * per; a++) h->twist[a] = h->base_twist[a] + pitch_deg[w];
+    }
+    DALM_CUDA(cudaMemcpy((void *)h->alm.wt, h->h_wt.data(), sizeof(TurbineDev) * T,
+                         cudaMemcpyHostToDevice));
+    DALM_CUDA(cudaMemcpy((void *)h->alm.twist, h->twist.data(), sizeof(double) * h->twist.size(),
+                         cudaMemcpyHostToDevice));
+    API_END(h)
+}
+
+int dalm_step(dalm_handle *h, int nsteps) {
+    API_BEGIN(h)
+    if (nsteps < 0) throw std::invalid_argument("nsteps < 0");
+    for (int n = 0; n < nsteps; n++) h->step_once();
+    h->sync_stats();
+    if (h->opt.check_finite && h->step > 1) {
+        if (!std::isfinite(h->h_diag->avg_div) || !std::isfinite(h->h_kst->err)) {
+            h->err = "non-finite state after step " + std::to_string(h->step - 1);
+            return DALM_ERR_NONFINITE;
+        }
+    }
+    API_END(h)
+}
+
+int dalm_run_stage(dalm_handle *h, int stage) {
+    API_BEGIN(h)
+    h->run_stage(stage);
+    h->sync_stats();
+    API_END(h)
+}
+
+int dalm_advance_clock(dalm_handle *h) {
+    API_BEGIN(h)
+    h->step++;
+    API_END(h)
+}
+
+int dalm_get_step_stats(dalm_handle *h, int64_t *step, int64_t *poisson_it, double *poisson_err,
+                        double *avg_div, double *max_cfl) {
+    API_BEGIN(h)
+    h->sync_stats();
+    if (step) *step = h->step;
+    if (poisson_it) *poisson_it = h->h_kst->it;
+    if (poisson_err) *poisson_err = h->h_kst->err;
+    if (avg_div) *avg_div = h->h_diag->avg_div;
+    if (max_cfl) *max_cfl = h->h_diag->max_cfl;
+    API_END(h)
+}
+
+int dalm_set_poisson(dalm_handle *h, int64_t max_it, double tol) {
+    API_BEGIN(h)
+    h->max_it = max_it;
+    h->tol = tol;
+    API_END(h)
+}
+
+int dalm_get_counts(dalm_handle *h, int64_t counts[5]) {
+    API_BEGIN(h)
+    if (!counts) throw std::invalid_argument("null output");
+    counts[0] = h->alm.wt_count;
+    counts[1] = h->alm.ap_count;
+    counts[2] = h->alm.blades;
+    counts[3] = h->alm.ap_per_blade;
+    counts[4] = h->alm.atk_count;
+    API_END(h)
+}
+
+int dalm_get_turbines(dalm_handle *h, double *thrust, double *torque, double *power) {
+    API_BEGIN(h)
+    h->sync_stats();
+    int T = h->alm.wt_count;
+    for (int w = 0; w < T; w++) {
+        double tq = h->h_wt_out[w], th = h->h_wt_out[T + w];
+        if (thrust) thrust[w] = th;
+        if (torque) torque[w] = tq;
+        if (power) power[w] = tq * fabs(h->h_wt[w].rot_speed);
+    }
+    API_END(h)
+}
+
+int dalm_get_points(dalm_handle *h, double *xyz, double *f, double *torque, double *thrust) {
+    API_BEGIN(h)
+    h->sync_stats();
+    int n = h->alm.ap_count;
+    if (n == 0) return DALM_OK;
+    if (xyz) DALM_CUDA(cudaMemcpy(xyz, h->alm.pt_xyz, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+    if (f) DALM_CUDA(cudaMemcpy(f, h->alm.pt_f, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+    if (torque) DALM_CUDA(cudaMemcpy(torque, h->alm.pt_torque, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (thrust) DALM_CUDA(cudaMemcpy(thrust, h->alm.pt_thrust, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    API_END(h)
+}
+
+int dalm_synchronize(dalm_handle *h) {
+    API_BEGIN(h)
+    h->sync_stats();
+    API_END(h)
+}
+
+int dalm_get_stream(dalm_handle *h, void **stream) {
+    API_BEGIN(h)
+    if (!stream) throw std::invalid_argument("null output");
+    *stream = (void *)h->stream;
+    API_END(h)
+}
+
+int dalm_get_timings(dalm_handle *h, double ms[7], int64_t *launches, int reset) {
+    API_BEGIN(h)
+    h->sync_stats();
+    if (ms)
+        for (int s = 0; s < 7; s++) ms[s] = h->stage_ms[s];
+    if (launches) *launches = h->launch_count;
+    if (reset) {
+        for (int s = 0; s < 7; s++) h->stage_ms[s] = 0;
+        for (int k = 0; k < KK_COUNT; k++) { h->kind_ms[k] = 0; h->kind_launches[k] = 0; }
+        h->launch_count = 0;
+    }
+    API_END(h)
+}
+
+int dalm_kernel_kinds(void) { return KK_COUNT; }
+
+int dalm_get_kernel_timing(dalm_handle *h, int index, const char **name, int64_t *launches,
+                           double *ms, double *bytes_per_launch) {
+    API_BEGIN(h)
+    if (index < 0 || index >= KK_COUNT) throw std::invalid_argument("kernel index out of range");
+    h->sync_stats();
+    if (name) *name = kKindNames[index];
+    if (launches) *launches = h->kind_launches[index];
+    if (ms) *ms = h->kind_ms[index];
+    if (bytes_per_launch) {
+        // algorithmic DRAM bytes: each persistent array read or written once
+        // per launch over interior cells (8-byte scalars)
+        double n = (double)h->g.ni() * h->g.nj() * h->g.nk();
+        double stored = (double)h->g.nx * h->g.ny * h->g.nz;
+        double fcells = h->fbox.empty() ? 0.0
+                        : (double)(h->fbox.hi[0] - h->fbox.lo[0]) * (h->fbox.hi[1] - h->fbox.lo[1]) *
+                              (h->fbox.hi[2] - h->fbox.lo[2]);
+        double s = 0;
+        switch (index) {
+        case KK_PREDICT: s = 9 * n + 3 * fcells + 6 * (stored - n); break;
+        case KK_FLUX_RHS: s = 7 * n; break;
+        case KK_PROJECT: s = 13 * n; break;
+        case KK_DIAG: s = 6 * n; break;
+        case KK_TAVG: s = 9 * stored; break;
+        case KK_ALM_PROJECT: s = 3 * fcells; break;
+        case KK_SOR_SWEEP: s = 2 * n; break;
+        case KK_RESIDUAL_NORM: s = (h->pcfg.method == PM_JACOBI ? 3 : 2) * n; break;
+        case KK_JACOBI_SWEEP: s = 3 * n; break;
+        case KK_BICG_INIT: s = 5 * n; break;
+        case KK_BICG_P: s = 5 * n; break;
+        case KK_BICG_Q: s = 3 * n; break;
+        case KK_BICG_S: s = 4 * n; break;
+        case KK_BICG_T: s = 3 * n; break;
+        case KK_BICG_XR: s = 8 * n; break;
+        default: s = 0; break;
+        }
+        *bytes_per_launch = 8.0 * s;
+    }
+    API_END(h)
+}
+
+}  // extern "C"

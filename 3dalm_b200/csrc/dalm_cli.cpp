@@ -1,0 +1,66 @@
+// Command-line driver: `dalm <case_dir> [--steps N] [--quiet]`.
+// Mirrors the reference's `solver <case_dir>` (src/solver.cpp:6-47): runs
+// steps 0..max_step (or N steps) and prints the per-step line
+// `step time it err avg_div max_cfl` (src/solver.h:1188-1190), then the
+// per-turbine thrust, torque and power.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <vector>
+
+#include "../../include/dalm.h"
+
+int main(int argc, char **argv) {
+    if (argc < 2) {
+        fprintf(stderr, "usage: %s <case_dir> [--steps N] [--quiet]\n", argv[0]);
+        return 2;
+    }
+    const char *dir = argv[1];
+    long long steps = -1;
+    bool quiet = false;
+    dalm_options opt;
+    dalm_default_options(&opt);
+    for (int a = 2; a < argc; a++) {
+        if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps = atoll(argv[++a]);
+        else if (!strcmp(argv[a], "--quiet")) quiet = true;
+    }
+    time_t t0 = time(0);
+    printf("START %s\n", ctime(&t0));
+    dalm_handle *h = nullptr;
+    int rc = dalm_create(dir, &opt, &h);
+    if (rc != DALM_OK) {
+        fprintf(stderr, "dalm_create failed (%d): %s\n", rc, dalm_last_error(nullptr));
+        return 1;
+    }
+    double dt = 0;
+    int64_t max_step = 0;
+    dalm_get_runtime(h, &dt, &max_step);
+    long long total = steps >= 0 ? steps : (long long)max_step + 1;
+    for (long long s = 0; s < total; s++) {
+        rc = dalm_step(h, 1);
+        if (rc != DALM_OK) {
+            fprintf(stderr, "dalm_step failed (%d): %s\n", rc, dalm_last_error(h));
+            dalm_destroy(h);
+            return 1;
+        }
+        int64_t step = 0, it = 0;
+        double err = 0, avg_div = 0, cfl = 0;
+        dalm_get_step_stats(h, &step, &it, &err, &avg_div, &cfl);
+        if (!quiet && step > 1)
+            printf("%lld %e %lld %e %e %e\n", (long long)(step - 1), dt * (double)(step - 1),
+                   (long long)it, err, avg_div, cfl);
+    }
+    int64_t counts[5];
+    dalm_get_counts(h, counts);
+    if (counts[0] > 0) {
+        std::vector<double> th(counts[0]), tq(counts[0]), pw(counts[0]);
+        dalm_get_turbines(h, th.data(), tq.data(), pw.data());
+        for (int64_t w = 0; w < counts[0]; w++)
+            printf("turbine %lld thrust %e torque %e power %e\n", (long long)w, th[w], tq[w], pw[w]);
+    }
+    dalm_destroy(h);
+    time_t t1 = time(0);
+    printf("END %s\n", ctime(&t1));
+    return 0;
+}

@@ -1,0 +1,350 @@
+// Pressure Poisson solvers (src/eq.h, src/mv.h) with matrix-free
+// coefficients and on-device loop control.
+//
+// Compiled with --fmad=false: each cell update keeps the reference's
+// operation order, so red-black SOR sweeps and Jacobi sweeps reproduce the
+// reference bit for bit; only the global dot products and norms are summed
+// in a different (deterministic, tree) order than the reference's serial
+// loops.
+#include <cfloat>
+
+#include "poisson.cuh"
+
+namespace dalm {
+
+namespace {
+
+struct Coef7 {
+    double ac, ae, aw, an, as, at, ab;
+};
+
+// Coefficients of cell (i,j,k) exactly as build_A assembles and scales them
+// (src/eq.h:720-794).
+__device__ __forceinline__ Coef7 coef7(const PoissonCoef &C, int i, int j, int k) {
+    double acu = 0.0 - C.ex[i];
+    acu = acu - C.aw_u[i];
+    acu = acu - C.an_u[j];
+    acu = acu - C.as_u[j];
+    acu = acu - C.at_u[k];
+    acu = acu - C.ab_u[k];
+    Coef7 a;
+    a.ac = acu / C.max_diag;
+    a.ae = C.ae[i]; a.aw = C.aw[i];
+    a.an = C.an[j]; a.as = C.as[j];
+    a.at = C.at[k]; a.ab = C.ab[k];
+    return a;
+}
+
+// ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb, left to right
+// (src/mv.h:87, 214; src/eq.h:36, 177).
+__device__ __forceinline__ double apply_a(const Grid &g, const Coef7 &a, const double *v,
+                                          long long c) {
+    return a.ac * v[c] + a.ae * v[c + g.sx] + a.aw * v[c - g.sx] + a.an * v[c + g.sy] +
+           a.as * v[c - g.sy] + a.at * v[c + 1] + a.ab * v[c - 1];
+}
+
+#define TILE_LOOP(T)                                                          \
+    for (long long tile = blockIdx.x; tile < (T).ntiles; tile += gridDim.x) { \
+        int i, j, k;                                                          \
+        if (!(T).cell(tile, i, j, k)) continue;                               \
+        long long c = g.at(i, j, k);
+
+#define TILE_END }
+
+__global__ void k_begin(KrylovState *st, long long max_it, double tol, double ncell) {
+    st->rho = 0; st->rho_old = 1; st->alpha = 1; st->omega = 1; st->beta = 0; st->err = 0;
+    st->ncell = ncell; st->tol = tol; st->it = 0; st->max_it = max_it; st->done = 0;
+}
+
+// Residual norm at the end of a SOR / Jacobi iteration and the stop rule
+// `while (it < max_it && err > tol)` (src/eq.h:297-305).
+__device__ __forceinline__ void finish_iteration(KrylovState *st, double sum_r2) {
+    st->err = sqrt(sum_r2) / sqrt(st->ncell);
+    st->it += 1;
+    if (!(st->it < st->max_it && st->err > st->tol)) st->done = 1;
+}
+
+// ---------------------------------------------------------------- SOR
+
+// sweep_sor_at_cell (src/eq.h:145-181), colour (i+j+k)%2 (offsets 0).
+__global__ void __launch_bounds__(TILE_THREADS)
+k_sor_sweep(Grid g, PoissonCoef C, Tiling T, double *x, const double *b, double w, int color,
+            const KrylovState *st) {
+    if (st->done) return;
+    TILE_LOOP(T)
+    if (((i + j + k) & 1) != color) continue;
+    Coef7 a = coef7(C, i, j, k);
+    double xc = x[c];
+    double rel = (b[c] - apply_a(g, a, x, c)) / a.ac;
+    x[c] = xc + w * rel;
+    TILE_END
+}
+
+// calc_residual + calc_l2_norm (src/mv.h:33-182) fused; when `copy_from`
+// is set the iterate lives there (Jacobi ping-pong) and is copied into x.
+__global__ void __launch_bounds__(TILE_THREADS)
+k_residual_norm(Grid g, PoissonCoef C, Tiling T, double *x, const double *copy_from,
+                const double *b, Partials<1> part, KrylovState *st) {
+    if (st->done) return;
+    const double *v = copy_from ? copy_from : x;
+    double acc = 0;
+    TILE_LOOP(T)
+    Coef7 a = coef7(C, i, j, k);
+    double r = b[c] - apply_a(g, a, v, c);
+    acc += r * r;
+    if (copy_from) x[c] = v[c];
+    TILE_END
+    double vals[1] = {acc};
+    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) finish_iteration(st, vals[0]);
+}
+
+// sweep_jacobi_at_cell (src/eq.h:6-39): out = in + (rhs - A in)/ac.
+__global__ void __launch_bounds__(TILE_THREADS)
+k_jacobi_sweep(Grid g, PoissonCoef C, Tiling T, double *out, const double *in, const double *rhs,
+               const KrylovState *st) {
+    if (st->done) return;
+    TILE_LOOP(T)
+    Coef7 a = coef7(C, i, j, k);
+    double rel = (rhs[c] - apply_a(g, a, in, c)) / a.ac;
+    out[c] = in[c] + rel;
+    TILE_END
+}
+
+// ------------------------------------------------------------ BiCGStab
+//
+// run_pbicgstab (src/eq.h:333-473).  One iteration is
+//   p-update (+ first Jacobi sweep from zero) -> PC sweeps -> q = A pp, <r0,q>
+//   -> s-update (+ first sweep) -> PC sweeps -> t = A ss, <t,s>, <t,t>
+//   -> x, r update, <r0,r>, <r,r>
+// Each reduction's last block computes the next scalar (alpha, omega, err,
+// rho, beta) on the device.
+
+// calc_residual, cpy_array(r0, r), fill(q, 0) and the first rho = <r0, r>
+// (src/eq.h:342-353).
+__global__ void __launch_bounds__(TILE_THREADS)
+k_bicg_init(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, Partials<1> part, KrylovState *st) {
+    double acc = 0;
+    TILE_LOOP(T)
+    Coef7 a = coef7(C, i, j, k);
+    double r = B.b[c] - apply_a(g, a, B.x, c);
+    B.r[c] = r;
+    B.r0[c] = r;
+    B.q[c] = 0;
+    acc += r * r;
+    TILE_END
+    double vals[1] = {acc};
+    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) {
+        st->rho = vals[0];
+        if (fabs(st->rho) < FLT_MIN) {
+            st->err = st->rho;
+            st->done = 1;
+        }
+    }
+}
+
+// p = r (it 0) or r + beta (p - omega q) (src/eq.h:355-365); with the
+// Jacobi preconditioner also the first sweep of run_jacobi_pc from a zero
+// guess, which is exactly 0 + (p - 0)/ac (src/eq.h:367-368); with SOR
+// the zero guess itself (src/eq.h:438).
+__global__ void __launch_bounds__(TILE_THREADS)
+k_bicg_p(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int first_sweep, const KrylovState *st) {
+    if (st->done) return;
+    const bool first = (st->it == 0);
+    const double beta = st->beta, omega = st->omega;
+    TILE_LOOP(T)
+    double pv = first ? B.r[c] : B.r[c] + beta * (B.pk[c] - omega * B.q[c]);
+    B.pk[c] = pv;
+    if (first_sweep) {
+        Coef7 a = coef7(C, i, j, k);
+        B.pp[c] = 0.0 + (pv - 0.0) / a.ac;
+    } else {
+        B.pp[c] = 0.0;
+    }
+    TILE_END
+}
+
+// s = r - alpha q (src/eq.h:373-377) with the same first-sweep fusion.
+__global__ void __launch_bounds__(TILE_THREADS)
+k_bicg_s(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int first_sweep, const KrylovState *st) {
+    if (st->done) return;
+    const double alpha = st->alpha;
+    TILE_LOOP(T)
+    double sv = B.r[c] - alpha * B.q[c];
+    B.s[c] = sv;
+    if (first_sweep) {
+        Coef7 a = coef7(C, i, j, k);
+        B.ss[c] = 0.0 + (sv - 0.0) / a.ac;
+    } else {
+        B.ss[c] = 0.0;
+    }
+    TILE_END
+}
+
+// q = A pp and <r0, q>; alpha = rho / <r0, q> (src/eq.h:369-371).
+__global__ void __launch_bounds__(TILE_THREADS)
+k_bicg_q(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ppf, Partials<1> part,
+         KrylovState *st) {
+    if (st->done) return;
+    double acc = 0;
+    TILE_LOOP(T)
+    Coef7 a = coef7(C, i, j, k);
+    double qv = apply_a(g, a, ppf, c);
+    B.q[c] = qv;
+    acc += B.r0[c] * qv;
+    TILE_END
+    double vals[1] = {acc};
+    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) st->alpha = st->rho / vals[0];
+}
+
+// t = A ss, <t, s>, <t, t>; omega = <t,s>/<t,t> (src/eq.h:381-383).
+__global__ void __launch_bounds__(TILE_THREADS)
+k_bicg_t(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ssf, Partials<2> part,
+         KrylovState *st) {
+    if (st->done) return;
+    double ts = 0, tt = 0;
+    TILE_LOOP(T)
+    Coef7 a = coef7(C, i, j, k);
+    double tv = apply_a(g, a, ssf, c);
+    B.t[c] = tv;
+    ts += tv * B.s[c];
+    tt += tv * tv;
+    TILE_END
+    double vals[2] = {ts, tt};
+    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) st->omega = vals[0] / vals[1];
+}
+
+// x += alpha pp + omega ss; r = s - omega t (src/eq.h:385-395); err =
+// ||r||/sqrt(N) and the loop test (src/eq.h:397-401); then the next
+// iteration's rho = <r0, r>, breakdown test and beta (src/eq.h:349-358).
+__global__ void __launch_bounds__(TILE_THREADS)
+k_bicg_xr(Grid g, Tiling T, PoissonBufs B, const double *ppf, const double *ssf,
+          Partials<2> part, KrylovState *st) {
+    if (st->done) return;
+    const double alpha = st->alpha, omega = st->omega;
+    double r0r = 0, rr = 0;
+    TILE_LOOP(T)
+    B.x[c] = B.x[c] + alpha * ppf[c] + omega * ssf[c];
+    double rv = B.s[c] - omega * B.t[c];
+    B.r[c] = rv;
+    r0r += B.r0[c] * rv;
+    rr += rv * rv;
+    TILE_END
+    double vals[2] = {r0r, rr};
+    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) {
+        st->rho_old = st->rho;
+        st->err = sqrt(vals[1]) / sqrt(st->ncell);
+        st->it += 1;
+        if (!(st->it < st->max_it && st->err > st->tol)) {
+            st->done = 1;
+        } else {
+            double rho = vals[0];
+            st->rho = rho;
+            if (fabs(rho) < FLT_MIN) {
+                st->err = rho;
+                st->done = 1;
+            } else {
+                st->beta = (rho / st->rho_old) * (st->alpha / st->omega);
+            }
+        }
+    }
+}
+
+Box interior_box(const Grid &g) {
+    return Box{{g.gc, g.gc, g.gc}, {g.nx - g.gc, g.ny - g.gc, g.nz - g.gc}};
+}
+
+}  // namespace
+
+void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it, double tol,
+                          double ncell) {
+    L.pre(KK_POISSON_BEGIN);
+    k_begin<<<1, 1, 0, L.s>>>(st, max_it, tol, ncell);
+    L.post(KK_POISSON_BEGIN);
+}
+
+void launch_sor_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                          const PoissonBufs &B, double relax, Partials<1> part, KrylovState *st) {
+    Tiling T = Tiling::make(interior_box(g));
+    for (int color = 0; color < 2; color++) {
+        L.pre(KK_SOR_SWEEP);
+        k_sor_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.b, relax, color, st);
+        L.post(KK_SOR_SWEEP);
+    }
+    L.pre(KK_RESIDUAL_NORM);
+    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, nullptr, B.b, part, st);
+    L.post(KK_RESIDUAL_NORM);
+}
+
+void launch_jacobi_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                             const PoissonBufs &B, Partials<1> part, KrylovState *st) {
+    Tiling T = Tiling::make(interior_box(g));
+    L.pre(KK_JACOBI_SWEEP);
+    k_jacobi_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.tp, B.x, B.b, st);
+    L.post(KK_JACOBI_SWEEP);
+    L.pre(KK_RESIDUAL_NORM);
+    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.tp, B.b, part, st);
+    L.post(KK_RESIDUAL_NORM);
+}
+
+void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                      const PoissonBufs &B, Partials<1> part, KrylovState *st) {
+    Tiling T = Tiling::make(interior_box(g));
+    L.pre(KK_BICG_INIT);
+    k_bicg_init<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, part, st);
+    L.post(KK_BICG_INIT);
+}
+
+// Applies the preconditioner to `rhs` with the first sweep already done
+// into `x` (Jacobi) or `x` zeroed (SOR); returns the buffer holding M^-1 rhs.
+static double *precondition(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                            const Tiling &T, const PoissonConfig &cfg, double *x, double *tmp,
+                            const double *rhs, const KrylovState *st) {
+    if (cfg.pc == PC_SOR) {
+        for (int n = 0; n < cfg.pc_sweeps; n++) {
+            for (int color = 0; color < 2; color++) {
+                L.pre(KK_SOR_SWEEP);
+                k_sor_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, x, rhs, cfg.pc_relax,
+                                                                 color, st);
+                L.post(KK_SOR_SWEEP);
+            }
+        }
+        return x;
+    }
+    double *cur = x, *nxt = tmp;
+    for (int n = 1; n < cfg.pc_sweeps; n++) {
+        L.pre(KK_JACOBI_SWEEP);
+        k_jacobi_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, nxt, cur, rhs, st);
+        L.post(KK_JACOBI_SWEEP);
+        double *t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    return cur;
+}
+
+void launch_bicg_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                           const PoissonBufs &B, const PoissonConfig &cfg, Partials<2> part,
+                           KrylovState *st) {
+    Tiling T = Tiling::make(interior_box(g));
+    int first = (cfg.pc == PC_JACOBI && cfg.pc_sweeps >= 1) ? 1 : 0;
+    Partials<1> part1{part.buf, part.ticket};
+    L.pre(KK_BICG_P);
+    k_bicg_p<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, first, st);
+    L.post(KK_BICG_P);
+    double *ppf = precondition(L, g, C, T, cfg, B.pp, B.tp, B.pk, st);
+    L.pre(KK_BICG_Q);
+    k_bicg_q<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ppf, part1, st);
+    L.post(KK_BICG_Q);
+    L.pre(KK_BICG_S);
+    k_bicg_s<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, first, st);
+    L.post(KK_BICG_S);
+    double *ssf = precondition(L, g, C, T, cfg, B.ss, B.ts, B.s, st);
+    L.pre(KK_BICG_T);
+    k_bicg_t<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ssf, part, st);
+    L.post(KK_BICG_T);
+    L.pre(KK_BICG_XR);
+    k_bicg_xr<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, T, B, ppf, ssf, part, st);
+    L.post(KK_BICG_XR);
+}
+
+}  // namespace dalm

@@ -1,0 +1,52 @@
+// Pressure Poisson solvers on the device (src/eq.h, src/mv.h).
+#pragma once
+
+#include "flow.cuh"
+
+namespace dalm {
+
+// Iteration state kept in device memory so the whole Krylov / SOR loop runs
+// without a host round trip per dot product; the host only polls `done`
+// between batches of enqueued iterations.
+struct KrylovState {
+    double rho, rho_old, alpha, omega, beta, err;
+    double ncell;     // interior cell count (effective_count)
+    double tol;
+    long long it, max_it;
+    int done;         // 1 once the reference loop would have exited
+    int pad;
+};
+
+struct PoissonBufs {
+    double *x;             // pressure (Cfd::p)
+    const double *b;       // right-hand side (Eq::b)
+    double *r, *r0, *pk, *q, *s, *t;   // Eq::r, r0, p, q, s, t
+    double *pp, *ss;       // preconditioned directions (Eq::pp, Eq::ss)
+    double *tp, *ts;       // Jacobi ping-pong partners of pp and ss
+};
+
+enum PoissonMethod { PM_SOR = 0, PM_BICG = 1, PM_JACOBI = 2 };
+enum PreconMethod { PC_JACOBI = 0, PC_SOR = 1 };
+
+struct PoissonConfig {
+    int method, pc;
+    double relax, pc_relax;
+    int pc_sweeps;
+};
+
+void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it, double tol,
+                          double ncell);
+// red-black SOR (src/eq.h:291-306): one iteration = red, black, residual norm
+void launch_sor_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                          const PoissonBufs &B, double relax, Partials<1> part, KrylovState *st);
+// standalone Jacobi: one sweep + residual norm
+void launch_jacobi_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                             const PoissonBufs &B, Partials<1> part, KrylovState *st);
+// BiCGStab (src/eq.h:333-473)
+void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                      const PoissonBufs &B, Partials<1> part, KrylovState *st);
+void launch_bicg_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                           const PoissonBufs &B, const PoissonConfig &cfg, Partials<2> part,
+                           KrylovState *st);
+
+}  // namespace dalm

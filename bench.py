@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the 3dalm time step on one B200 per rank.
+
+Workload: the 3-turbine case, 512x256x128 interior cells (16.78 M) over a
+20x5x5 domain stretched toward the ground, turbines at x = 4, 9, 14 (yaw 0,
+10, 0 deg, 3 blades x 32 points, R = 0.5, TSR 6), log-law inflow
+(u* = 0.05, z0 = 1e-3) + seeded 8% Gaussian perturbation, Re = 1e4,
+Cs = 0.1, dt = 1e-3, minmod MUSCL, Jacobi(3)-preconditioned BiCGStab to
+1e-8.  Synthetic inputs (no dataset exists for this solver); every field is
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+A step is Solver::main_loop_once: predictor, face flux + Poisson RHS, the
+Poisson solve to tolerance, projection + BCs, actuator line.  Metric:
+Mcell-steps/s = interior cells x steps / time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the case on
+its own GPU (the path has no exchange step on one domain): weak scaling, no
+collective on the data path; the time is the max over ranks.
+"""
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s"
+CASE = "c4"
+
+# Poisson iteration counts of the first integrating steps of this workload
+# (seed 0), measured by this benchmark's GPU arm; the FP64 GPU path and the
+# reference take the same number of iterations (tests/test_gpu_parity.py),
+# so the reference arm's per-step time model uses them.
+C4_ITERATIONS = None  # filled from a measured run; None -> use the sample's own count
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", default=CASE)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` at this workload from the committed
+    ncu summary (profiles/traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)[CASE][kernel]["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError, TypeError):
+        return None
+
+
+def make_case(name, tmp):
+    cg = importlib.import_module("3dalm_b200.casegen")
+    spec = cg.config(name, steps=100000)
+    mesh = cg.write_case(spec, tmp)
+    return spec, mesh, cg.initial_velocity(spec, mesh), cg.inflow_profile(spec, mesh)
+
+
+# ------------------------------------------------------------------ CPU side
+
+def cpu_sample(kind_pref="reference", iterations=None, poisson_cap=40):
+    """Time the CPU oracle (the reference compiled from its own sources when
+    available, else the C restatement) stage by stage on a bounded sample:
+    the same 3-turbine case at 128x64x32 cells (262,144), one integrating
+    step with the Poisson solve capped at `poisson_cap` iterations.  The
+    per-cell stage costs, the per-cell-per-iteration Poisson cost and the
+    per-cell-per-blade-point projection cost are combined into the time of
+    one full 512x256x128 step with `iterations` Poisson iterations (serial,
+    one core).  Returns (Mcell-steps/s, kind, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    kind = "reference" if (kind_pref == "reference" and O.reference_available()) else "port"
+    if kind == "port" and not os.path.exists(O.LIB_C):
+        O.build()
+    cg = importlib.import_module("3dalm_b200.casegen")
+    full = cg.config(CASE)
+    spec = cg.config(CASE, n=(128, 64, 32), steps=10)
+    with tempfile.TemporaryDirectory() as d:
+        mesh = cg.write_case(spec, d)
+        o = O.Reference(d) if kind == "reference" else O.CRestatement(d)
+        prof = cg.inflow_profile(spec, mesh)
+        o.set_inflow_profile(prof)
+        o.set_state(cg.initial_velocity(spec, mesh))
+        o.advance_clock()
+        o.set_poisson(poisson_cap, 0.0)
+        t = []
+        for st in range(6):
+            t0 = time.perf_counter()
+            o.stage(st)
+            t.append(time.perf_counter() - t0)
+        it = o.stats()["it"]
+        n_pts = o.turbine_count() * 3 * spec.points_per_blade
+        o.close()
+    n_s = spec.n[0] * spec.n[1] * spec.n[2]
+    n_f = full.n[0] * full.n[1] * full.n[2]
+    per_cell = (t[0] + t[1] + t[3] + t[5]) / n_s
+    per_iter = t[2] / (it * n_s)
+    per_cell_point = t[4] / (n_s * n_pts)
+    its = iterations if iterations else it
+    step_time = n_f * (per_cell + its * per_iter) + n_f * n_pts * per_cell_point
+    desc = (f"{'reference (oracle/_ref)' if kind == 'reference' else 'C restatement'} serial, "
+            f"stage-timed on the same case at 128x64x32 ({n_s} cells, {n_pts} blade points, "
+            f"Poisson capped at {it} iterations); per-cell, per-cell-iteration and "
+            f"per-cell-point costs scaled to 512x256x128 with {its:.1f} Poisson iterations/step")
+    return n_f / step_time / 1e6, kind, desc, sum(t)
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    iters = None
+    if C4_ITERATIONS:
+        iters = statistics.mean(C4_ITERATIONS[:max(1, args.steps)])
+    vals = []
+    for n in range(args.warmup + args.steps):
+        v, kind, desc, secs = cpu_sample("reference", iters)
+        if n >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 16777216 / (value * 1e6) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "3-turbine 512x256x128 LES step (Jacobi-BiCGStab 1e-8, log-law "
+                               "inflow, 288 blade points)", "case": CASE},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
+                         "sample": desc},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU side
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    pkg = importlib.import_module("3dalm_b200")
+    tmp = tempfile.mkdtemp(prefix=f"dalm_bench_r{rank}_")
+    spec, mesh, U0, prof = make_case(args.case, tmp)
+    s = pkg.Solver(tmp, device=local, profile=True)
+    s.set_inflow_profile(prof)
+    s.set_state(U0)
+    n_int = spec.n[0] * spec.n[1] * spec.n[2]
+    s.step(max(args.warmup, 1))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # ---- device-resident timed region
+    stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
+    s.timings(reset=True)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    s.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    its = []
+    for _ in range(args.steps):
+        s.step(1)
+        its.append(s.stats()["it"])
+    e1.record(stream)
+    e1.synchronize()
+    s.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    kt = s.kernel_timings()
+    stage_ms, launches = s.timings()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n_int * args.steps * world / (ms / 1e3) / 1e6
+
+    # ---- end to end through the public API with host (pinned) buffers
+    e2e_steps = max(1, args.e2e_steps)
+    U_h = torch.empty(s._shape(3), dtype=torch.float64).pin_memory().numpy()
+    p_h = torch.empty(s._shape(1), dtype=torch.float64).pin_memory().numpy()
+    s.field("U", out=U_h)
+    s.field("p", out=p_h)
+    barrier()
+    torch.cuda.synchronize()
+    s.synchronize()
+    w0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.set_field("U", U_h)
+        s.set_field("p", p_h)
+        s.step(1)
+        s.field("U", out=U_h)
+        s.field("p", out=p_h)
+        s.stats()
+    s.synchronize()
+    e2e_s = time.perf_counter() - w0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = n_int * e2e_steps * world / e2e_s / 1e6
+    h2d = U_h.nbytes + p_h.nbytes
+
+    # ---- roofline of the dominant kernel
+    dom = max((k for k in kt if kt[k]["launches"] > 0 and kt[k]["bytes_per_launch"] > 0),
+              key=lambda k: kt[k]["ms"])
+    d = kt[dom]
+    per_launch_s = d["ms"] / d["launches"] / 1e3
+    achieved = d["bytes_per_launch"] / per_launch_s / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic(dom)
+    n_launch = sum(v["launches"] for v in kt.values())
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded log-law + 8% Gaussian initial field, generated case files)",
+        "config": {"workload": "3-turbine 512x256x128 LES step (Jacobi(3)-BiCGStab to 1e-8, "
+                               "log-law inflow, 288 blade points)",
+                   "case": args.case, "precision": "FP64", "cells": n_int,
+                   "poisson_iterations": its, "parallelism": f"replicas x{world}",
+                   "l2": "every field > 126 MB L2 (141 MB per scalar field); no flush"},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": h2d, "steps": e2e_steps,
+                "how": "per step: dalm_set_field(U,p) from pinned host, dalm_step(1), "
+                       "dalm_get_field(U,p) to pinned host, dalm_get_step_stats; wall clock"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": d["bytes_per_launch"],
+                     "launch_us": per_launch_s * 1e6, "launches": d["launches"],
+                     "share_of_kernel_time": d["ms"] / max(1e-9, sum(v["ms"] for v in kt.values()))},
+        "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+        "gpu_launches": n_launch,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, desc, secs = cpu_sample("reference", statistics.mean(its))
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
+                                "sample": desc, "sample_seconds": secs}
+    s.finalize()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
