@@ -52,7 +52,7 @@ class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("limiter", C.c_int), ("device", C.c_int),
                 ("time_average", C.c_int), ("check_finite", C.c_int),
                 ("poisson_batch", C.c_int), ("use_graphs", C.c_int), ("profile", C.c_int),
-                ("reserved", C.c_int * 8)]
+                ("reference_sums", C.c_int), ("reserved", C.c_int * 7)]
 
 
 _PD = C.POINTER(C.c_double)
@@ -93,7 +93,7 @@ class Solver:
 
     def __init__(self, case_dir: str | None = None, precision: int = FP64, device: int = 0,
                  time_average: bool = True, profile: bool = False, poisson_batch: int = 0,
-                 limiter: int = MINMOD):
+                 limiter: int = MINMOD, reference_sums: bool = False):
         self.lib = load_library()
         self.h = C.c_void_p()
         self.opt = Options()
@@ -104,6 +104,7 @@ class Solver:
         self.opt.time_average = int(time_average)
         self.opt.profile = int(profile)
         self.opt.poisson_batch = poisson_batch
+        self.opt.reference_sums = int(reference_sums)
         if case_dir is not None:
             self.initialize(case_dir)
 

@@ -33,7 +33,7 @@ const char *kKindNames[KK_COUNT] = {
     "alm_points", "alm_sums", "alm_project",
     "sor_sweep", "residual_norm", "jacobi_sweep",
     "bicg_init", "bicg_p", "bicg_q", "bicg_s", "bicg_t", "bicg_xr",
-    "poisson_begin", "layout"};
+    "poisson_begin", "layout", "seq_sum"};
 
 struct EventPair {
     cudaEvent_t a, b;
@@ -241,6 +241,7 @@ struct dalm_handle {
         pcfg.relax = cs.relax;
         pcfg.pc_relax = cs.pc_relax;
         pcfg.pc_sweeps = (int)cs.pc_max_it;
+        pcfg.reference_sums = opt.reference_sums ? 1 : 0;
         partial = dalloc<double>((size_t)L.blocks * 4);
         ticket = dalloc<unsigned int>(1);
         d_kst = dalloc<KrylovState>(1);
@@ -259,6 +260,8 @@ struct dalm_handle {
         for (int m = 0; m < 3; m++) P.uin[m] = cs.uin[m];
         P.prof = nullptr;
         P.fbox = fbox;
+        P.reference_sums = opt.reference_sums ? 1 : 0;
+        P.filter2 = build_filter();
 
         init_alm();
 
@@ -268,6 +271,21 @@ struct dalm_handle {
             for (int m = 0; m < 3; m++) launch_fill(L, U[b][m], g.total, cs.uin[m]);
         refresh_after_state(DALM_SET_APPLY_UBC | DALM_SET_RECOMPUTE_JU, nullptr);
         DALM_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // (Cs * cbrt(dx dy dz))^2 per interior cell with the host libm's cbrt,
+    // the factor calc_nut_at_cell applies (src/cfd.h:804, 823-824).
+    const double *build_filter() {
+        std::vector<double> f((size_t)g.total, 0.0);
+        for (int i = g.gc; i < g.nx - g.gc; i++)
+            for (int j = g.gc; j < g.ny - g.gc; j++)
+                for (int k = g.gc; k < g.nz - g.gc; k++) {
+                    double volume = cs.dx[i] * cs.dy[j] * cs.dz[k];
+                    double filter = cbrt(volume);
+                    double v = cs.cs * filter;
+                    f[(size_t)g.at(i, j, k)] = v * v;
+                }
+        return upload(f);
     }
 
     // build_A (src/eq.h:701-798) as per-axis arrays; see PoissonCoef.
@@ -372,16 +390,17 @@ struct dalm_handle {
         if (pcfg.method == PM_BICG) {
             launch_bicg_iteration(L, g, coef, pb, pcfg, Partials<2>{partial, ticket}, d_kst);
         } else if (pcfg.method == PM_SOR) {
-            launch_sor_iteration(L, g, coef, pb, pcfg.relax, Partials<1>{partial, ticket}, d_kst);
+            launch_sor_iteration(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
         } else {
-            launch_jacobi_iteration(L, g, coef, pb, Partials<1>{partial, ticket}, d_kst);
+            launch_jacobi_iteration(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
         }
     }
     void stage_poisson() {
         StageTimer t(this, DALM_STAGE_POISSON);
         double ncell = (double)g.ni() * g.nj() * g.nk();
         launch_poisson_begin(L, d_kst, max_it, tol, ncell);
-        if (pcfg.method == PM_BICG) launch_bicg_init(L, g, coef, pb, Partials<1>{partial, ticket}, d_kst);
+        if (pcfg.method == PM_BICG)
+            launch_bicg_init(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
         long long issued = 0;
         long long batch = opt.poisson_batch > 0 ? opt.poisson_batch
                                                 : std::max<long long>(4, last_it > 0 ? last_it : 16);
@@ -639,6 +658,7 @@ void dalm_default_options(dalm_options *opt) {
     opt->poisson_batch = 0;
     opt->use_graphs = 1;
     opt->profile = 0;
+    opt->reference_sums = 0;
 }
 
 int dalm_create(const char *case_dir, const dalm_options *opt, dalm_handle **out) {

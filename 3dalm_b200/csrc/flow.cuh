@@ -35,12 +35,50 @@ struct StepParams {
     double uin[3];
     const double *prof;  // inflow profile [ny][nz][3] on the device, or null
     Box fbox;            // cells where the ALM force may be non-zero
+    // (Cs * cbrt(dx dy dz))^2 per interior cell, computed once on the host
+    // with the same libm cbrt the reference calls (src/cfd.h:804, 823-824)
+    const double *filter2;
+    // 1: global sums in the reference's serial (i,j,k) order
+    // (warp_serial_sums) instead of the parallel tree
+    int reference_sums;
 };
 
 struct DiagState {
     double div2, max_cfl, avg_div;  // sum div^2, max cfl, ||div||/sqrt(N)
     double ncell;
 };
+
+// Sums in the reference's serial order.  The reference accumulates every
+// global sum with one loop over interior cells, i outer, k inner
+// (src/mv.h:8-55, src/cfd.h:1109-1141); a parallel tree sum rounds
+// differently, and BiCGStab's iteration count and iterates are sensitive to
+// that rounding.  This helper reproduces the serial order exactly and is run
+// by a single warp: the warp loads 32 consecutive k values at a time, then
+// folds them into the running sum one term at a time in lane order.  Every
+// lane ends with the same total.
+template <int N, typename Term>
+__device__ inline void warp_serial_sums(const Grid &g, Term term, double (&total)[N]) {
+    int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int m = 0; m < N; m++) total[m] = 0;
+    int kend = g.nz - g.gc;
+    for (int i = g.gc; i < g.nx - g.gc; i++)
+        for (int j = g.gc; j < g.ny - g.gc; j++)
+            for (int k0 = g.gc; k0 < kend; k0 += 32) {
+                int k = k0 + lane;
+                double t[N];
+                if (k < kend) {
+                    term(g.at(i, j, k), t);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < N; m++) t[m] = 0;
+                }
+                int n = kend - k0 < 32 ? kend - k0 : 32;
+                for (int l = 0; l < n; l++)
+#pragma unroll
+                    for (int m = 0; m < N; m++) total[m] = total[m] + __shfl_sync(0xffffffffu, t[m], l);
+            }
+}
 
 // ---- flow kernels (flow_fp64.cu) ----
 void launch_predict(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,

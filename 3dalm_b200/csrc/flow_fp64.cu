@@ -39,15 +39,16 @@ __device__ __forceinline__ void muscl_axis(double fmm, double fm, double fc, dou
 __device__ __forceinline__ double sq(double v) { return v * v; }
 
 // Smagorinsky viscosity at (i,j,k) from the velocity (src/cfd.h:786-825).
+// The filter factor (Cs cbrt(dx dy dz))^2 comes precomputed per cell.
 __device__ __forceinline__ double smagorinsky(const StepParams &P, Vec3<const double> U, int i,
                                               int j, int k) {
     const Grid &g = P.g;
+    long long c = g.at(i, j, k);
     long long e = g.at(i + 1, j, k), w = g.at(i - 1, j, k), n = g.at(i, j + 1, k),
-              s = g.at(i, j - 1, k), t = g.at(i, j, k + 1), b = g.at(i, j, k - 1);
+              s = g.at(i, j - 1, k), t = c + 1, b = c - 1;
     double dxew = P.m.x[i + 1] - P.m.x[i - 1];
     double dyns = P.m.y[j + 1] - P.m.y[j - 1];
     double dztb = P.m.z[k + 1] - P.m.z[k - 1];
-    double volume = P.m.dx[i] * P.m.dy[j] * P.m.dz[k];
     double dudx = (U.c[0][e] - U.c[0][w]) / dxew;
     double dudy = (U.c[0][n] - U.c[0][s]) / dyns;
     double dudz = (U.c[0][t] - U.c[0][b]) / dztb;
@@ -60,8 +61,7 @@ __device__ __forceinline__ double smagorinsky(const StepParams &P, Vec3<const do
     double s1 = 2 * sq(dudx), s2 = 2 * sq(dvdy), s3 = 2 * sq(dwdz);
     double s4 = sq(dudy + dvdx), s5 = sq(dudz + dwdx), s6 = sq(dvdz + dwdy);
     double shear = sqrt(s1 + s2 + s3 + s4 + s5 + s6);
-    double filter = cbrt(volume);
-    return sq(P.cs * filter) * shear;
+    return P.filter2[c] * shear;
 }
 
 __device__ __forceinline__ bool interior(const Grid &g, int i, int j, int k) {
@@ -301,6 +301,7 @@ k_project(StepParams P, Tiling T, Vec3<double> U, Vec3<double> JUin, Vec3<double
             cfl = local > cfl ? local : cfl;
         }
     }
+    if (P.reference_sums) return;  // k_seq_diag sums in the reference's order
     double v[2] = {div2, cfl};
     if (grid_reduce<2>(v, 2u, part) && threadIdx.x == 0) {
         diag->div2 = v[0];
@@ -309,22 +310,34 @@ k_project(StepParams P, Tiling T, Vec3<double> U, Vec3<double> JUin, Vec3<double
     }
 }
 
+// divergence of cell c from the face fluxes (src/cfd.h:1093-1105) and the
+// cell CFL number (src/cfd.h:1126-1130)
+__device__ __forceinline__ double cell_div(const StepParams &P, Vec3<const double> JU, int i,
+                                           int j, int k) {
+    const Grid &g = P.g;
+    long long c = g.at(i, j, k);
+    double J = P.m.dx[i] * P.m.dy[j] * P.m.dz[k];
+    return (JU.c[0][c] - JU.c[0][g.at(i - 1, j, k)] + JU.c[1][c] - JU.c[1][g.at(i, j - 1, k)] +
+            JU.c[2][c] - JU.c[2][c - 1]) / J;
+}
+__device__ __forceinline__ double cell_cfl(const StepParams &P, Vec3<const double> U, int i,
+                                           int j, int k) {
+    long long c = P.g.at(i, j, k);
+    return fabs(U.c[0][c]) * P.dt / P.m.dx[i] + fabs(U.c[1][c]) * P.dt / P.m.dy[j] +
+           fabs(U.c[2][c]) * P.dt / P.m.dz[k];
+}
+
 // Diagnostics alone (after set_state): sum div^2 and max CFL.
 __global__ void __launch_bounds__(TILE_THREADS)
 k_diag(StepParams P, Tiling T, Vec3<const double> U, Vec3<const double> JU, Partials<2> part,
        DiagState *diag) {
-    const Grid &g = P.g;
     double div2 = 0, cfl = 0;
     for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
         int i, j, k;
         if (!T.cell(tile, i, j, k)) continue;
-        long long c = g.at(i, j, k);
-        double J = P.m.dx[i] * P.m.dy[j] * P.m.dz[k];
-        double d = (JU.c[0][c] - JU.c[0][g.at(i - 1, j, k)] + JU.c[1][c] -
-                    JU.c[1][g.at(i, j - 1, k)] + JU.c[2][c] - JU.c[2][c - 1]) / J;
+        double d = cell_div(P, JU, i, j, k);
         div2 += d * d;
-        double local = fabs(U.c[0][c]) * P.dt / P.m.dx[i] + fabs(U.c[1][c]) * P.dt / P.m.dy[j] +
-                       fabs(U.c[2][c]) * P.dt / P.m.dz[k];
+        double local = cell_cfl(P, U, i, j, k);
         cfl = local > cfl ? local : cfl;
     }
     double v[2] = {div2, cfl};
@@ -332,6 +345,42 @@ k_diag(StepParams P, Tiling T, Vec3<const double> U, Vec3<const double> JU, Part
         diag->div2 = v[0];
         diag->max_cfl = v[1];
         diag->avg_div = sqrt(v[0]) / sqrt(diag->ncell);
+    }
+}
+
+// The same diagnostics summed in the reference's serial order by one warp:
+// calc_l2_norm(div) (src/mv.h:33-55) and calc_max_cfl (src/cfd.h:1109-1141).
+__global__ void k_seq_diag(StepParams P, Vec3<const double> U, Vec3<const double> JU,
+                           DiagState *diag) {
+    const Grid &g = P.g;
+    double tot[2];
+    warp_serial_sums<2>(
+        g,
+        [&](long long c, double (&t)[2]) {
+            long long r = c - g.off;
+            int i = (int)(r / g.sx), j = (int)((r % g.sx) / g.sy), k = (int)(r % g.sy);
+            double d = cell_div(P, JU, i, j, k);
+            t[0] = d * d;
+            t[1] = 0;
+        },
+        tot);
+    // max is exact in any order
+    double cfl = 0;
+    int lane = threadIdx.x & 31;
+    for (int i = g.gc; i < g.nx - g.gc; i++)
+        for (int j = g.gc; j < g.ny - g.gc; j++)
+            for (int k = g.gc + lane; k < g.nz - g.gc; k += 32) {
+                double local = cell_cfl(P, U, i, j, k);
+                cfl = local > cfl ? local : cfl;
+            }
+    for (int o = 16; o > 0; o >>= 1) {
+        double other = __shfl_down_sync(0xffffffffu, cfl, o);
+        cfl = other > cfl ? other : cfl;
+    }
+    if (lane == 0) {
+        diag->div2 = tot[0];
+        diag->max_cfl = cfl;
+        diag->avg_div = sqrt(tot[0]) / sqrt(diag->ncell);
     }
 }
 
@@ -559,6 +608,12 @@ void launch_project(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
     L.pre(KK_PROJECT);
     k_project<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju_in, ju_out, p, part, diag);
     L.post(KK_PROJECT);
+    if (P.reference_sums) {
+        L.pre(KK_DIAG);
+        k_seq_diag<<<1, 32, 0, L.s>>>(P, {{u.c[0], u.c[1], u.c[2]}},
+                                      {{ju_out.c[0], ju_out.c[1], ju_out.c[2]}}, diag);
+        L.post(KK_DIAG);
+    }
 }
 
 void launch_velocity_bc(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
@@ -572,7 +627,10 @@ void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                  Vec3<const double> ju, Partials<2> part, DiagState *diag) {
     Tiling T = Tiling::make(interior_box(P.g));
     L.pre(KK_DIAG);
-    k_diag<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju, part, diag);
+    if (P.reference_sums)
+        k_seq_diag<<<1, 32, 0, L.s>>>(P, u, ju, diag);
+    else
+        k_diag<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju, part, diag);
     L.post(KK_DIAG);
 }
 

@@ -82,9 +82,10 @@ k_sor_sweep(Grid g, PoissonCoef C, Tiling T, double *x, const double *b, double 
 
 // calc_residual + calc_l2_norm (src/mv.h:33-182) fused; when `copy_from`
 // is set the iterate lives there (Jacobi ping-pong) and is copied into x.
+// With `rstore` the residual is stored (reference-order sums read it back).
 __global__ void __launch_bounds__(TILE_THREADS)
 k_residual_norm(Grid g, PoissonCoef C, Tiling T, double *x, const double *copy_from,
-                const double *b, Partials<1> part, KrylovState *st) {
+                const double *b, double *rstore, Partials<1> part, KrylovState *st) {
     if (st->done) return;
     const double *v = copy_from ? copy_from : x;
     double acc = 0;
@@ -92,8 +93,10 @@ k_residual_norm(Grid g, PoissonCoef C, Tiling T, double *x, const double *copy_f
     Coef7 a = coef7(C, i, j, k);
     double r = b[c] - apply_a(g, a, v, c);
     acc += r * r;
+    if (rstore) rstore[c] = r;
     if (copy_from) x[c] = v[c];
     TILE_END
+    if (rstore) return;
     double vals[1] = {acc};
     if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) finish_iteration(st, vals[0]);
 }
@@ -119,10 +122,74 @@ k_jacobi_sweep(Grid g, PoissonCoef C, Tiling T, double *out, const double *in, c
 // Each reduction's last block computes the next scalar (alpha, omega, err,
 // rho, beta) on the device.
 
+
+// ---- finishers: the scalar updates after each global sum -----------------
+
+// rho = <r0, r> and the breakdown test (src/eq.h:349-353)
+__device__ __forceinline__ void fin_init(KrylovState *st, double r0r) {
+    st->rho = r0r;
+    if (fabs(st->rho) < FLT_MIN) {
+        st->err = st->rho;
+        st->done = 1;
+    }
+}
+// alpha = rho / <r0, q> (src/eq.h:371)
+__device__ __forceinline__ void fin_q(KrylovState *st, double r0q) { st->alpha = st->rho / r0q; }
+// omega = <t, s> / <t, t> (src/eq.h:383)
+__device__ __forceinline__ void fin_t(KrylovState *st, double ts, double tt) { st->omega = ts / tt; }
+// rhoold = rho; err = ||r||/sqrt(N); it++; loop test; next rho, breakdown
+// test and beta (src/eq.h:397-401, 349-358)
+__device__ __forceinline__ void fin_xr(KrylovState *st, double r0r, double rr) {
+    st->rho_old = st->rho;
+    st->err = sqrt(rr) / sqrt(st->ncell);
+    st->it += 1;
+    if (!(st->it < st->max_it && st->err > st->tol)) {
+        st->done = 1;
+    } else {
+        st->rho = r0r;
+        if (fabs(r0r) < FLT_MIN) {
+            st->err = r0r;
+            st->done = 1;
+        } else {
+            st->beta = (r0r / st->rho_old) * (st->alpha / st->omega);
+        }
+    }
+}
+
+enum SeqSite { SEQ_RESIDUAL = 0, SEQ_INIT = 1, SEQ_Q = 2, SEQ_T = 3, SEQ_XR = 4 };
+
+// One warp: the sums of one site in the reference's serial order, then its
+// finisher (reference-order-sum mode).
+__global__ void k_seq(Grid g, int site, const double *a0, const double *b0, const double *a1,
+                      const double *b1, KrylovState *st) {
+    if (site != SEQ_INIT && st->done) return;
+    double tot[2];
+    if (a1) {
+        warp_serial_sums<2>(g, [&](long long c, double (&t)[2]) {
+            t[0] = a0[c] * b0[c];
+            t[1] = a1[c] * b1[c];
+        }, tot);
+    } else {
+        double one[1];
+        warp_serial_sums<1>(g, [&](long long c, double (&t)[1]) { t[0] = a0[c] * b0[c]; }, one);
+        tot[0] = one[0];
+        tot[1] = 0;
+    }
+    if (threadIdx.x != 0) return;
+    switch (site) {
+    case SEQ_RESIDUAL: finish_iteration(st, tot[0]); break;
+    case SEQ_INIT: fin_init(st, tot[0]); break;
+    case SEQ_Q: fin_q(st, tot[0]); break;
+    case SEQ_T: fin_t(st, tot[0], tot[1]); break;
+    case SEQ_XR: fin_xr(st, tot[0], tot[1]); break;
+    }
+}
+
 // calc_residual, cpy_array(r0, r), fill(q, 0) and the first rho = <r0, r>
 // (src/eq.h:342-353).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_init(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, Partials<1> part, KrylovState *st) {
+k_bicg_init(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int seq, Partials<1> part,
+            KrylovState *st) {
     double acc = 0;
     TILE_LOOP(T)
     Coef7 a = coef7(C, i, j, k);
@@ -132,14 +199,9 @@ k_bicg_init(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, Partials<1> part, Kr
     B.q[c] = 0;
     acc += r * r;
     TILE_END
+    if (seq) return;
     double vals[1] = {acc};
-    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) {
-        st->rho = vals[0];
-        if (fabs(st->rho) < FLT_MIN) {
-            st->err = st->rho;
-            st->done = 1;
-        }
-    }
+    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) fin_init(st, vals[0]);
 }
 
 // p = r (it 0) or r + beta (p - omega q) (src/eq.h:355-365); with the
@@ -182,8 +244,8 @@ k_bicg_s(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int first_sweep, const 
 
 // q = A pp and <r0, q>; alpha = rho / <r0, q> (src/eq.h:369-371).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_q(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ppf, Partials<1> part,
-         KrylovState *st) {
+k_bicg_q(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ppf, int seq,
+         Partials<1> part, KrylovState *st) {
     if (st->done) return;
     double acc = 0;
     TILE_LOOP(T)
@@ -192,14 +254,15 @@ k_bicg_q(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ppf, Part
     B.q[c] = qv;
     acc += B.r0[c] * qv;
     TILE_END
+    if (seq) return;
     double vals[1] = {acc};
-    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) st->alpha = st->rho / vals[0];
+    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) fin_q(st, vals[0]);
 }
 
 // t = A ss, <t, s>, <t, t>; omega = <t,s>/<t,t> (src/eq.h:381-383).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_t(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ssf, Partials<2> part,
-         KrylovState *st) {
+k_bicg_t(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ssf, int seq,
+         Partials<2> part, KrylovState *st) {
     if (st->done) return;
     double ts = 0, tt = 0;
     TILE_LOOP(T)
@@ -209,15 +272,15 @@ k_bicg_t(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ssf, Part
     ts += tv * B.s[c];
     tt += tv * tv;
     TILE_END
+    if (seq) return;
     double vals[2] = {ts, tt};
-    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) st->omega = vals[0] / vals[1];
+    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) fin_t(st, vals[0], vals[1]);
 }
 
-// x += alpha pp + omega ss; r = s - omega t (src/eq.h:385-395); err =
-// ||r||/sqrt(N) and the loop test (src/eq.h:397-401); then the next
-// iteration's rho = <r0, r>, breakdown test and beta (src/eq.h:349-358).
+// x += alpha pp + omega ss; r = s - omega t (src/eq.h:385-395) with
+// <r0, r> and <r, r> for the finisher.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_xr(Grid g, Tiling T, PoissonBufs B, const double *ppf, const double *ssf,
+k_bicg_xr(Grid g, Tiling T, PoissonBufs B, const double *ppf, const double *ssf, int seq,
           Partials<2> part, KrylovState *st) {
     if (st->done) return;
     const double alpha = st->alpha, omega = st->omega;
@@ -229,28 +292,20 @@ k_bicg_xr(Grid g, Tiling T, PoissonBufs B, const double *ppf, const double *ssf,
     r0r += B.r0[c] * rv;
     rr += rv * rv;
     TILE_END
+    if (seq) return;
     double vals[2] = {r0r, rr};
-    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) {
-        st->rho_old = st->rho;
-        st->err = sqrt(vals[1]) / sqrt(st->ncell);
-        st->it += 1;
-        if (!(st->it < st->max_it && st->err > st->tol)) {
-            st->done = 1;
-        } else {
-            double rho = vals[0];
-            st->rho = rho;
-            if (fabs(rho) < FLT_MIN) {
-                st->err = rho;
-                st->done = 1;
-            } else {
-                st->beta = (rho / st->rho_old) * (st->alpha / st->omega);
-            }
-        }
-    }
+    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) fin_xr(st, vals[0], vals[1]);
 }
 
 Box interior_box(const Grid &g) {
     return Box{{g.gc, g.gc, g.gc}, {g.nx - g.gc, g.ny - g.gc, g.nz - g.gc}};
+}
+
+void seq_launch(const LaunchCtx &L, const Grid &g, int site, const double *a0, const double *b0,
+                const double *a1, const double *b1, KrylovState *st) {
+    L.pre(KK_SEQ_SUM);
+    k_seq<<<1, 32, 0, L.s>>>(g, site, a0, b0, a1, b1, st);
+    L.post(KK_SEQ_SUM);
 }
 
 }  // namespace
@@ -263,35 +318,43 @@ void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it,
 }
 
 void launch_sor_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
-                          const PoissonBufs &B, double relax, Partials<1> part, KrylovState *st) {
+                          const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
+                          KrylovState *st) {
     Tiling T = Tiling::make(interior_box(g));
     for (int color = 0; color < 2; color++) {
         L.pre(KK_SOR_SWEEP);
-        k_sor_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.b, relax, color, st);
+        k_sor_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.b, cfg.relax, color, st);
         L.post(KK_SOR_SWEEP);
     }
+    double *rs = cfg.reference_sums ? B.r : nullptr;
     L.pre(KK_RESIDUAL_NORM);
-    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, nullptr, B.b, part, st);
+    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, nullptr, B.b, rs, part, st);
     L.post(KK_RESIDUAL_NORM);
+    if (rs) seq_launch(L, g, SEQ_RESIDUAL, B.r, B.r, nullptr, nullptr, st);
 }
 
 void launch_jacobi_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
-                             const PoissonBufs &B, Partials<1> part, KrylovState *st) {
+                             const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
+                             KrylovState *st) {
     Tiling T = Tiling::make(interior_box(g));
     L.pre(KK_JACOBI_SWEEP);
     k_jacobi_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.tp, B.x, B.b, st);
     L.post(KK_JACOBI_SWEEP);
+    double *rs = cfg.reference_sums ? B.r : nullptr;
     L.pre(KK_RESIDUAL_NORM);
-    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.tp, B.b, part, st);
+    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.tp, B.b, rs, part, st);
     L.post(KK_RESIDUAL_NORM);
+    if (rs) seq_launch(L, g, SEQ_RESIDUAL, B.r, B.r, nullptr, nullptr, st);
 }
 
 void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
-                      const PoissonBufs &B, Partials<1> part, KrylovState *st) {
+                      const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
+                      KrylovState *st) {
     Tiling T = Tiling::make(interior_box(g));
     L.pre(KK_BICG_INIT);
-    k_bicg_init<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, part, st);
+    k_bicg_init<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, cfg.reference_sums, part, st);
     L.post(KK_BICG_INIT);
+    if (cfg.reference_sums) seq_launch(L, g, SEQ_INIT, B.r0, B.r, nullptr, nullptr, st);
 }
 
 // Applies the preconditioner to `rhs` with the first sweep already done
@@ -327,24 +390,28 @@ void launch_bicg_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef 
                            KrylovState *st) {
     Tiling T = Tiling::make(interior_box(g));
     int first = (cfg.pc == PC_JACOBI && cfg.pc_sweeps >= 1) ? 1 : 0;
+    int seq = cfg.reference_sums;
     Partials<1> part1{part.buf, part.ticket};
     L.pre(KK_BICG_P);
     k_bicg_p<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, first, st);
     L.post(KK_BICG_P);
     double *ppf = precondition(L, g, C, T, cfg, B.pp, B.tp, B.pk, st);
     L.pre(KK_BICG_Q);
-    k_bicg_q<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ppf, part1, st);
+    k_bicg_q<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ppf, seq, part1, st);
     L.post(KK_BICG_Q);
+    if (seq) seq_launch(L, g, SEQ_Q, B.r0, B.q, nullptr, nullptr, st);
     L.pre(KK_BICG_S);
     k_bicg_s<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, first, st);
     L.post(KK_BICG_S);
     double *ssf = precondition(L, g, C, T, cfg, B.ss, B.ts, B.s, st);
     L.pre(KK_BICG_T);
-    k_bicg_t<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ssf, part, st);
+    k_bicg_t<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ssf, seq, part, st);
     L.post(KK_BICG_T);
+    if (seq) seq_launch(L, g, SEQ_T, B.t, B.s, B.t, B.t, st);
     L.pre(KK_BICG_XR);
-    k_bicg_xr<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, T, B, ppf, ssf, part, st);
+    k_bicg_xr<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, T, B, ppf, ssf, seq, part, st);
     L.post(KK_BICG_XR);
+    if (seq) seq_launch(L, g, SEQ_XR, B.r0, B.r, B.r, B.r, st);
 }
 
 }  // namespace dalm

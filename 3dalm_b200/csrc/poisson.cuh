@@ -32,19 +32,23 @@ struct PoissonConfig {
     int method, pc;
     double relax, pc_relax;
     int pc_sweeps;
+    int reference_sums;  // 1: global sums in the reference's serial order
 };
 
 void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it, double tol,
                           double ncell);
 // red-black SOR (src/eq.h:291-306): one iteration = red, black, residual norm
 void launch_sor_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
-                          const PoissonBufs &B, double relax, Partials<1> part, KrylovState *st);
+                          const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
+                          KrylovState *st);
 // standalone Jacobi: one sweep + residual norm
 void launch_jacobi_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
-                             const PoissonBufs &B, Partials<1> part, KrylovState *st);
+                             const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
+                             KrylovState *st);
 // BiCGStab (src/eq.h:333-473)
 void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
-                      const PoissonBufs &B, Partials<1> part, KrylovState *st);
+                      const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
+                      KrylovState *st);
 void launch_bicg_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                            const PoissonBufs &B, const PoissonConfig &cfg, Partials<2> part,
                            KrylovState *st);

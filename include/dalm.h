@@ -93,7 +93,12 @@ typedef struct {
     int use_graphs;       /* 1: replay iteration batches as CUDA graphs  */
     int profile;          /* 1: time every kernel launch with CUDA events
                              (dalm_get_kernel_timings)                   */
-    int reserved[8];
+    int reference_sums;   /* 1: every global sum (Krylov dots, norms,
+                             divergence norm) in the reference's serial
+                             cell order instead of a parallel tree; with it
+                             the FP64 step reproduces the reference's
+                             rounding (slow: for parity checks)          */
+    int reserved[7];
 } dalm_options;
 
 /* Fills *opt with the defaults (FP64, minmod, device 0, time average on,

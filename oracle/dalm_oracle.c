@@ -44,6 +44,7 @@ struct dalm_oracle {
     int64_t it, max_it, pc_max_it;
     double err, tol, relax, pc_relax;
     double avg_div, max_cfl;
+    int sum_order; /* 0: the reference's serial sums; 1: pairwise (test only) */
     /* runtime (src/solver.h:176-205) */
     int64_t step, max_step, tavg_count;
     double tavg_start_time;
@@ -396,14 +397,38 @@ static void matvec(dalm_oracle *o, const double *x, double *y) {
     const double *a;
     FOR_INTERIOR(o) { y[ID(o, i, j, k)] = stencil_sum(o, x, i, j, k, &a); }
 }
-/* calc_inner_product, src/mv.h:8-31 */
+/* Pairwise (recursive halving) sum, used only by the summation-order
+ * sensitivity mode below. */
+static double pairwise_sum(const double *v, int64_t n) {
+    if (n <= 8) {
+        double s = 0;
+        for (int64_t i = 0; i < n; i++) s += v[i];
+        return s;
+    }
+    int64_t h = n / 2;
+    return pairwise_sum(v, h) + pairwise_sum(v + h, n - h);
+}
+
+/* calc_inner_product, src/mv.h:8-31.  With sum_order == 1 (a test-only
+ * perturbation, never the default) the same products are summed pairwise
+ * instead of serially, to measure how sensitive the solver is to the
+ * summation order alone. */
 static double dot(const dalm_oracle *o, const double *a, const double *b) {
+    if (o->sum_order == 1) {
+        double *v = malloc(sizeof(double) * (size_t)o->len);
+        int64_t n = 0;
+        FOR_INTERIOR(o) { v[n++] = a[ID(o, i, j, k)] * b[ID(o, i, j, k)]; }
+        double s = pairwise_sum(v, n);
+        free(v);
+        return s;
+    }
     double tot = 0;
     FOR_INTERIOR(o) { tot += a[ID(o, i, j, k)] * b[ID(o, i, j, k)]; }
     return tot;
 }
 /* calc_l2_norm, src/mv.h:33-55 */
 static double l2norm(const dalm_oracle *o, const double *v) {
+    if (o->sum_order == 1) return sqrt(dot(o, v, v));
     double tot = 0;
     FOR_INTERIOR(o) { tot += sq(v[ID(o, i, j, k)]); }
     return sqrt(tot);
@@ -1002,6 +1027,8 @@ void oracle_set_poisson(dalm_oracle *o, int64_t max_it, double tol) {
     o->max_it = max_it;
     o->tol = tol;
 }
+
+void oracle_set_sum_order(dalm_oracle *o, int mode) { o->sum_order = mode; }
 
 void oracle_turbines(const dalm_oracle *o, double *torque, double *thrust) {
     for (int64_t w = 0; w < o->wt_count; w++) {

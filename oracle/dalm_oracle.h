@@ -76,6 +76,9 @@ void oracle_get_field(const dalm_oracle *o, int which, double *out);
 void oracle_set_field(dalm_oracle *o, int which, const double *in);
 void oracle_stats(const dalm_oracle *o, int64_t *ints, double *reals);
 void oracle_set_poisson(dalm_oracle *o, int64_t max_it, double tol);
+/* Test-only: 1 sums dot products pairwise instead of serially (measures the
+ * solver's sensitivity to summation order); 0 (default) is the reference. */
+void oracle_set_sum_order(dalm_oracle *o, int mode);
 void oracle_turbines(const dalm_oracle *o, double *torque, double *thrust);
 void oracle_points(const dalm_oracle *o, double *xyz, double *f, double *torque,
                    double *thrust);

@@ -310,7 +310,7 @@ class CRestatement(_Base):
             for n in ("destroy", "size", "mesh", "matrix", "set_inflow_profile",
                       "set_turbine_params", "set_state", "stage", "step", "advance_clock",
                       "get_field", "set_field", "stats", "set_poisson", "turbines", "points",
-                      "point_tables", "max_diag"):
+                      "point_tables", "max_diag", "set_sum_order"):
                 getattr(lib, "oracle_" + n).argtypes = None
             CRestatement._lib = lib
         self.lib = CRestatement._lib
@@ -323,6 +323,10 @@ class CRestatement(_Base):
         self._point_count = (self._turbine_count * int(wt["number of blades"]) *
                              self.case.points_per_blade) if wt else 0
         self._atk_count = len(wt["blade"]["attack angle"]) if wt else 0
+
+    def set_sum_order(self, mode: int):
+        """Test-only: 1 sums dot products pairwise instead of serially."""
+        self.lib.oracle_set_sum_order(self.h, int(mode))
 
     def close(self):
         if self.h:
