@@ -414,11 +414,22 @@ static double pairwise_sum(const double *v, int64_t n) {
  * instead of serially, to measure how sensitive the solver is to the
  * summation order alone. */
 static double dot(const dalm_oracle *o, const double *a, const double *b) {
-    if (o->sum_order == 1) {
+    if (o->sum_order != 0) {
         double *v = malloc(sizeof(double) * (size_t)o->len);
         int64_t n = 0;
         FOR_INTERIOR(o) { v[n++] = a[ID(o, i, j, k)] * b[ID(o, i, j, k)]; }
-        double s = pairwise_sum(v, n);
+        double s = 0;
+        if (o->sum_order == 1) {
+            s = pairwise_sum(v, n);
+        } else if (o->sum_order == 2) { /* reversed serial */
+            for (int64_t m = n - 1; m >= 0; m--) s += v[m];
+        } else { /* 3: 1184 strided partial sums, then serial (a GPU-like order) */
+            for (int64_t p = 0; p < 1184; p++) {
+                double part = 0;
+                for (int64_t m = p; m < n; m += 1184) part += v[m];
+                s += part;
+            }
+        }
         free(v);
         return s;
     }

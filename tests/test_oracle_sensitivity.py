@@ -2,45 +2,56 @@
 global dot products, measured on the oracle itself (CPU).
 
 The reference sums every dot product and norm serially over cells
-(src/mv.h:8-55).  Summing the very same products pairwise instead, with every
-other operation unchanged, already changes BiCGStab's iteration counts and
-moves the pressure by ~1e-5 relative within ten steps: the Krylov iterates
-are only determined to the solver tolerance, and which iterate is reached
-depends on rounding.  A GPU tree reduction is one more such order.  This test
-records that envelope; tests/test_gpu_parity.py uses it for the fast GPU
-mode and demands bit-identical results in the reference-order-sum mode."""
+(src/mv.h:8-55).  Summing the very same products in another order (pairwise,
+reversed, or as 1184 strided partial sums like a GPU grid), with every other
+operation unchanged, already changes BiCGStab's iteration counts by up to
+~22% and moves the pressure by ~2e-4 relative within ten steps: the Krylov
+iterates are only determined to the solver tolerance, and which iterate is
+reached depends on rounding.  A GPU tree reduction is one more such order.
+This test measures that spread and checks it against ENVELOPE, the bound the
+fast GPU mode is held to in tests/test_gpu_parity.py (the reference-order-sum
+GPU mode is held to bit identity instead)."""
 import numpy as np
+import pytest
 
 import oracle as O
 
-# the envelope the GPU fast mode is held to (tests/test_gpu_parity.py)
-ENVELOPE = {"it_abs": 3, "it_rel": 0.10, "U": 1e-7, "p": 1e-3}
+# measured worst case over orders 1-3 and the tiny cases: iterations 21.5%,
+# u,v,w 1.4e-8, p 2.0e-4 (tiny-turbine / tiny-loglaw, ten steps)
+ENVELOPE = {"it_abs": 3, "it_rel": 0.25, "U": 1e-7, "p": 1e-3}
 
 
-def run(d, spec, mesh, U0, prof, order, steps=10):
+def run(d, U0, prof, order, steps=10):
     o = O.CRestatement(d)
     o.set_sum_order(order)
     if prof is not None:
         o.set_inflow_profile(prof)
     o.set_state(U0)
-    its = []
+    its, Us, ps = [], [], []
     for _ in range(steps + 1):
         o.step(1)
         its.append(o.stats()["it"])
-    out = its, o.field("U"), o.field("p")
+        Us.append(o.field("U"))
+        ps.append(o.field("p"))
     o.close()
-    return out
+    return its, Us, ps
 
 
-def test_summation_order_alone_changes_iterations(make_case):
-    spec, mesh, d, U0, prof = make_case("tiny-bicg")
-    its0, U0r, p0 = run(d, spec, mesh, U0, prof, 0)
-    its1, U1, p1 = run(d, spec, mesh, U0, prof, 1)
-    assert its0 != its1, "expected the iteration counts to depend on summation order"
-    du = np.linalg.norm(U1 - U0r) / np.linalg.norm(U0r)
-    dp = np.linalg.norm(p1 - p0) / np.linalg.norm(p0)
-    assert du > 1e-12 and dp > 1e-8
-    # and the perturbation stays inside the envelope used for the GPU fast mode
-    for a, b in zip(its0, its1):
-        assert abs(a - b) <= max(ENVELOPE["it_abs"], ENVELOPE["it_rel"] * a)
-    assert du <= ENVELOPE["U"] and dp <= ENVELOPE["p"]
+@pytest.mark.parametrize("name", ["tiny-bicg", "tiny-turbine"])
+def test_summation_order_alone_moves_the_solution(make_case, name):
+    spec, mesh, d, U0, prof = make_case(name)
+    base = run(d, U0, prof, 0)
+    spread = {"it": 0.0, "U": 0.0, "p": 0.0}
+    differs = False
+    for order in (1, 2, 3):
+        its, Us, ps = run(d, U0, prof, order)
+        differs |= its != base[0]
+        for n in range(1, len(its)):
+            a, b = its[n], base[0][n]
+            assert abs(a - b) <= max(ENVELOPE["it_abs"], ENVELOPE["it_rel"] * b), (order, n, a, b)
+            spread["it"] = max(spread["it"], abs(a - b) / b)
+            spread["U"] = max(spread["U"], np.linalg.norm(Us[n] - base[1][n]) / np.linalg.norm(base[1][n]))
+            spread["p"] = max(spread["p"], np.linalg.norm(ps[n] - base[2][n]) / np.linalg.norm(base[2][n]))
+    assert differs, "expected the iteration counts to depend on the summation order"
+    assert spread["U"] > 1e-12 and spread["p"] > 1e-8
+    assert spread["U"] <= ENVELOPE["U"] and spread["p"] <= ENVELOPE["p"]
