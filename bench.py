@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default=CASE)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2,
+                    help="steps of the end-to-end (host buffer) measurement; 0 skips it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -276,30 +277,32 @@ def run_ours(args):
     value = n_int * args.steps * world / (ms / 1e3) / 1e6
 
     # ---- end to end through the public API with host (pinned) buffers
-    e2e_steps = max(1, args.e2e_steps)
-    U_h = torch.empty(s._shape(3), dtype=torch.float64).pin_memory().numpy()
-    p_h = torch.empty(s._shape(1), dtype=torch.float64).pin_memory().numpy()
-    s.field("U", out=U_h)
-    s.field("p", out=p_h)
-    barrier()
-    torch.cuda.synchronize()
-    s.synchronize()
-    w0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        s.set_field("U", U_h)
-        s.set_field("p", p_h)
-        s.step(1)
+    e2e_steps = args.e2e_steps
+    e2e_value, h2d = None, 0
+    if e2e_steps > 0:
+        U_h = torch.empty(s._shape(3), dtype=torch.float64).pin_memory().numpy()
+        p_h = torch.empty(s._shape(1), dtype=torch.float64).pin_memory().numpy()
         s.field("U", out=U_h)
         s.field("p", out=p_h)
-        s.stats()
-    s.synchronize()
-    e2e_s = time.perf_counter() - w0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = n_int * e2e_steps * world / e2e_s / 1e6
-    h2d = U_h.nbytes + p_h.nbytes
+        barrier()
+        torch.cuda.synchronize()
+        s.synchronize()
+        w0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            s.set_field("U", U_h)
+            s.set_field("p", p_h)
+            s.step(1)
+            s.field("U", out=U_h)
+            s.field("p", out=p_h)
+            s.stats()
+        s.synchronize()
+        e2e_s = time.perf_counter() - w0
+        if world > 1:
+            t = torch.tensor([e2e_s], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_value = n_int * e2e_steps * world / e2e_s / 1e6
+        h2d = U_h.nbytes + p_h.nbytes
 
     # ---- roofline of the dominant kernel
     dom = max((k for k in kt if kt[k]["launches"] > 0 and kt[k]["bytes_per_launch"] > 0),
