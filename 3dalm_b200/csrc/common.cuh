@@ -96,6 +96,48 @@ struct Tiling {
     }
 };
 
+// Column segments: the box is cut into (32 k) x (8 j) columns, and each
+// column into i-chunks of `ich` planes.  One block of 256 threads owns one
+// segment; each thread marches along i through its chunk, so neighbours in i
+// rotate through registers and every index is 32-bit arithmetic done once
+// per block.  Segment u: column = u % ncol, chunk = u / ncol.
+struct Segments {
+    Box box;
+    int ntk, ntj, ncol, nchunk, ich;
+    int count;
+    __host__ static Segments make(const Box &b, int target_blocks) {
+        Segments s;
+        s.box = b;
+        s.ntk = (b.hi[2] - b.lo[2] + TK - 1) / TK;
+        s.ntj = (b.hi[1] - b.lo[1] + TJ - 1) / TJ;
+        s.ncol = s.ntk * s.ntj;
+        int ni = b.hi[0] - b.lo[0];
+        if (b.empty()) {
+            s.ncol = s.nchunk = s.count = 0;
+            s.ich = 1;
+            return s;
+        }
+        // enough segments to fill the GPU, at most 32 planes per chunk
+        int want_chunks = (target_blocks + s.ncol - 1) / s.ncol;
+        s.ich = (ni + want_chunks - 1) / want_chunks;
+        if (s.ich < 1) s.ich = 1;
+        if (s.ich > 32) s.ich = 32;
+        s.nchunk = (ni + s.ich - 1) / s.ich;
+        s.count = s.ncol * s.nchunk;
+        return s;
+    }
+    // this thread's (k, j) and the segment's [i0, i1); false when (k, j) is
+    // outside the box
+    __device__ bool column(int u, int &i0, int &i1, int &j, int &k) const {
+        int col = u % ncol, chunk = u / ncol;
+        k = box.lo[2] + (col % ntk) * TK + (int)(threadIdx.x & 31);
+        j = box.lo[1] + (col / ntk) * TJ + (int)(threadIdx.x >> 5);
+        i0 = box.lo[0] + chunk * ich;
+        i1 = min(i0 + ich, box.hi[0]);
+        return k < box.hi[2] && j < box.hi[1];
+    }
+};
+
 // ---- deterministic reductions ---------------------------------------------
 //
 // Each block reduces its values in a fixed order (warp shuffles, then warps

@@ -242,7 +242,8 @@ struct dalm_handle {
         pcfg.pc_relax = cs.pc_relax;
         pcfg.pc_sweeps = (int)cs.pc_max_it;
         pcfg.reference_sums = opt.reference_sums ? 1 : 0;
-        partial = dalloc<double>((size_t)L.blocks * 4);
+        pcfg.seg = poisson_segments(g, sm_count);
+        partial = dalloc<double>((size_t)std::max(L.blocks, pcfg.seg.count) * 4);
         ticket = dalloc<unsigned int>(1);
         d_kst = dalloc<KrylovState>(1);
         d_diag = dalloc<DiagState>(1);
@@ -323,6 +324,9 @@ struct dalm_handle {
         coef.an = upload(an); coef.as = upload(as);
         coef.at = upload(at); coef.ab = upload(ab);
         coef.max_diag = md;
+        std::vector<double> xpart(NX, 0);
+        for (int64_t i = 0; i < NX; i++) xpart[i] = (0.0 - ex[i]) - awu[i];
+        coef.xpart = upload(xpart);
     }
 
     void init_alm() {
@@ -401,10 +405,15 @@ struct dalm_handle {
         launch_poisson_begin(L, d_kst, max_it, tol, ncell);
         if (pcfg.method == PM_BICG)
             launch_bicg_init(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
+        // Enqueue iterations in batches and poll the device's `done` flag in
+        // between.  The first batch stops a little short of the previous
+        // solve's count; later batches grow with the count so far.  Kernels
+        // enqueued after convergence return at once.
         long long issued = 0;
         long long batch = opt.poisson_batch > 0 ? opt.poisson_batch
-                                                : std::max<long long>(4, last_it > 0 ? last_it : 16);
+                                                : (last_it > 12 ? last_it - 8 : 4);
         while (true) {
+            batch = std::min<long long>(batch, std::max<long long>(1, max_it - issued));
             for (long long n = 0; n < batch; n++) enqueue_poisson_iteration();
             issued += batch;
             DALM_CUDA(cudaMemcpyAsync(h_kst, d_kst, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream));
@@ -413,7 +422,7 @@ struct dalm_handle {
             if (issued > max_it + 1)
                 throw std::runtime_error("Poisson loop did not stop at its iteration limit");
             batch = opt.poisson_batch > 0 ? opt.poisson_batch
-                                          : std::max<long long>(4, std::min<long long>(64, issued / 8));
+                                          : std::max<long long>(4, std::min<long long>(64, issued / 16));
         }
         last_it = h_kst->it;
     }

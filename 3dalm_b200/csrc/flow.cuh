@@ -25,6 +25,7 @@ struct MeshDev {
 struct PoissonCoef {
     const double *ex, *aw_u, *an_u, *as_u, *at_u, *ab_u;
     const double *ae, *aw, *an, *as, *at, *ab;
+    const double *xpart;  // (0 - ex[i]) - aw_u[i]: the first two steps of a_c
     double max_diag;
 };
 

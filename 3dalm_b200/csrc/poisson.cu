@@ -3,9 +3,14 @@
 //
 // Compiled with --fmad=false: each cell update keeps the reference's
 // operation order, so red-black SOR sweeps and Jacobi sweeps reproduce the
-// reference bit for bit; only the global dot products and norms are summed
-// in a different (deterministic, tree) order than the reference's serial
-// loops.
+// reference bit for bit.  Global dot products and norms are summed either
+// by a deterministic parallel tree (default) or, in reference-order-sum
+// mode, serially in the reference's cell order (k_seq).
+//
+// Kernels walk column segments (Segments): a block owns 32 (k) x 8 (j)
+// cells of a column and marches through a chunk of i-planes, rotating the
+// west / centre / east values of the stencil operand through registers, so
+// each plane of the operand is read once from DRAM per sweep.
 #include <cfloat>
 
 #include "poisson.cuh"
@@ -14,42 +19,47 @@ namespace dalm {
 
 namespace {
 
-struct Coef7 {
-    double ac, ae, aw, an, as, at, ab;
+// Per-thread (fixed j, k) part of the coefficients: everything except the
+// i-dependent terms, hoisted out of the i march.
+struct ColumnCoef {
+    double an, as, at, ab;          // scaled (A[id][3..6] of the reference)
+    double an_u, as_u, at_u, ab_u;  // unscaled, for the diagonal
 };
 
-// Coefficients of cell (i,j,k) exactly as build_A assembles and scales them
-// (src/eq.h:720-794).
-__device__ __forceinline__ Coef7 coef7(const PoissonCoef &C, int i, int j, int k) {
-    double acu = 0.0 - C.ex[i];
-    acu = acu - C.aw_u[i];
-    acu = acu - C.an_u[j];
-    acu = acu - C.as_u[j];
-    acu = acu - C.at_u[k];
-    acu = acu - C.ab_u[k];
-    Coef7 a;
-    a.ac = acu / C.max_diag;
-    a.ae = C.ae[i]; a.aw = C.aw[i];
-    a.an = C.an[j]; a.as = C.as[j];
-    a.at = C.at[k]; a.ab = C.ab[k];
-    return a;
+__device__ __forceinline__ ColumnCoef column_coef(const PoissonCoef &C, int j, int k) {
+    ColumnCoef cc;
+    cc.an = C.an[j]; cc.as = C.as[j]; cc.at = C.at[k]; cc.ab = C.ab[k];
+    cc.an_u = C.an_u[j]; cc.as_u = C.as_u[j]; cc.at_u = C.at_u[k]; cc.ab_u = C.ab_u[k];
+    return cc;
+}
+
+// a_c of cell (i, j, k) exactly as build_A assembles and scales it
+// (src/eq.h:720-794): ((((((0 - ex) - aw) - an) - as) - at) - ab) / max_diag,
+// the first two subtractions precomputed per i in C.xpart.
+__device__ __forceinline__ double diag(const PoissonCoef &C, const ColumnCoef &cc, int i) {
+    double acu = C.xpart[i] - cc.an_u;
+    acu = acu - cc.as_u;
+    acu = acu - cc.at_u;
+    acu = acu - cc.ab_u;
+    return acu / C.max_diag;
 }
 
 // ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb, left to right
-// (src/mv.h:87, 214; src/eq.h:36, 177).
-__device__ __forceinline__ double apply_a(const Grid &g, const Coef7 &a, const double *v,
-                                          long long c) {
-    return a.ac * v[c] + a.ae * v[c + g.sx] + a.aw * v[c - g.sx] + a.an * v[c + g.sy] +
-           a.as * v[c - g.sy] + a.at * v[c + 1] + a.ab * v[c - 1];
+// (src/mv.h:87, 214; src/eq.h:36, 177); xw, xc, xe come from registers.
+__device__ __forceinline__ double apply_a(const Grid &g, double ac, double ae, double aw,
+                                          const ColumnCoef &cc, double xw, double xc, double xe,
+                                          const double *v, long long c) {
+    return ac * xc + ae * xe + aw * xw + cc.an * v[c + g.sy] + cc.as * v[c - g.sy] +
+           cc.at * v[c + 1] + cc.ab * v[c - 1];
 }
 
-#define TILE_LOOP(T)                                                          \
-    for (long long tile = blockIdx.x; tile < (T).ntiles; tile += gridDim.x) { \
-        int i, j, k;                                                          \
-        if (!(T).cell(tile, i, j, k)) continue;                               \
-        long long c = g.at(i, j, k);
+#define SEGMENT_LOOP(S)                                                   \
+    for (int u = blockIdx.x; u < (S).count; u += gridDim.x) {             \
+        int i0, i1, j, k;                                                 \
+        if (!(S).column(u, i0, i1, j, k)) continue;                       \
+        long long c0 = g.at(i0, j, k);
 
-#define TILE_END }
+#define SEGMENT_END }
 
 __global__ void k_begin(KrylovState *st, long long max_it, double tol, double ncell) {
     st->rho = 0; st->rho_old = 1; st->alpha = 1; st->omega = 1; st->beta = 0; st->err = 0;
@@ -67,35 +77,53 @@ __device__ __forceinline__ void finish_iteration(KrylovState *st, double sum_r2)
 // ---------------------------------------------------------------- SOR
 
 // sweep_sor_at_cell (src/eq.h:145-181), colour (i+j+k)%2 (offsets 0).
+// The colour's cells are updated in place; their neighbours all have the
+// other colour, so the registers rotated along i are never stale.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_sor_sweep(Grid g, PoissonCoef C, Tiling T, double *x, const double *b, double w, int color,
+k_sor_sweep(Grid g, PoissonCoef C, Segments S, double *x, const double *b, double w, int color,
             const KrylovState *st) {
     if (st->done) return;
-    TILE_LOOP(T)
-    if (((i + j + k) & 1) != color) continue;
-    Coef7 a = coef7(C, i, j, k);
-    double xc = x[c];
-    double rel = (b[c] - apply_a(g, a, x, c)) / a.ac;
-    x[c] = xc + w * rel;
-    TILE_END
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    double xw = x[c - g.sx], xc = x[c];
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double xe = x[c + g.sx];
+        if (((i + j + k) & 1) == color) {
+            double ac = diag(C, cc, i);
+            double rel = (b[c] - apply_a(g, ac, C.ae[i], C.aw[i], cc, xw, xc, xe, x, c)) / ac;
+            xc = xc + w * rel;
+            x[c] = xc;
+        }
+        xw = xc;
+        xc = xe;
+    }
+    SEGMENT_END
 }
 
 // calc_residual + calc_l2_norm (src/mv.h:33-182) fused; when `copy_from`
 // is set the iterate lives there (Jacobi ping-pong) and is copied into x.
 // With `rstore` the residual is stored (reference-order sums read it back).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_residual_norm(Grid g, PoissonCoef C, Tiling T, double *x, const double *copy_from,
+k_residual_norm(Grid g, PoissonCoef C, Segments S, double *x, const double *copy_from,
                 const double *b, double *rstore, Partials<1> part, KrylovState *st) {
     if (st->done) return;
     const double *v = copy_from ? copy_from : x;
     double acc = 0;
-    TILE_LOOP(T)
-    Coef7 a = coef7(C, i, j, k);
-    double r = b[c] - apply_a(g, a, v, c);
-    acc += r * r;
-    if (rstore) rstore[c] = r;
-    if (copy_from) x[c] = v[c];
-    TILE_END
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    double xw = v[c - g.sx], xc = v[c];
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double xe = v[c + g.sx];
+        double r = b[c] - apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, v, c);
+        acc += r * r;
+        if (rstore) rstore[c] = r;
+        if (copy_from) x[c] = xc;
+        xw = xc;
+        xc = xe;
+    }
+    SEGMENT_END
     if (rstore) return;
     double vals[1] = {acc};
     if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) finish_iteration(st, vals[0]);
@@ -103,14 +131,22 @@ k_residual_norm(Grid g, PoissonCoef C, Tiling T, double *x, const double *copy_f
 
 // sweep_jacobi_at_cell (src/eq.h:6-39): out = in + (rhs - A in)/ac.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_jacobi_sweep(Grid g, PoissonCoef C, Tiling T, double *out, const double *in, const double *rhs,
+k_jacobi_sweep(Grid g, PoissonCoef C, Segments S, double *out, const double *in, const double *rhs,
                const KrylovState *st) {
     if (st->done) return;
-    TILE_LOOP(T)
-    Coef7 a = coef7(C, i, j, k);
-    double rel = (rhs[c] - apply_a(g, a, in, c)) / a.ac;
-    out[c] = in[c] + rel;
-    TILE_END
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    double xw = in[c - g.sx], xc = in[c];
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double xe = in[c + g.sx];
+        double ac = diag(C, cc, i);
+        double rel = (rhs[c] - apply_a(g, ac, C.ae[i], C.aw[i], cc, xw, xc, xe, in, c)) / ac;
+        out[c] = xc + rel;
+        xw = xc;
+        xc = xe;
+    }
+    SEGMENT_END
 }
 
 // ------------------------------------------------------------ BiCGStab
@@ -121,7 +157,6 @@ k_jacobi_sweep(Grid g, PoissonCoef C, Tiling T, double *out, const double *in, c
 //   -> x, r update, <r0,r>, <r,r>
 // Each reduction's last block computes the next scalar (alpha, omega, err,
 // rho, beta) on the device.
-
 
 // ---- finishers: the scalar updates after each global sum -----------------
 
@@ -188,17 +223,24 @@ __global__ void k_seq(Grid g, int site, const double *a0, const double *b0, cons
 // calc_residual, cpy_array(r0, r), fill(q, 0) and the first rho = <r0, r>
 // (src/eq.h:342-353).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_init(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int seq, Partials<1> part,
+k_bicg_init(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int seq, Partials<1> part,
             KrylovState *st) {
     double acc = 0;
-    TILE_LOOP(T)
-    Coef7 a = coef7(C, i, j, k);
-    double r = B.b[c] - apply_a(g, a, B.x, c);
-    B.r[c] = r;
-    B.r0[c] = r;
-    B.q[c] = 0;
-    acc += r * r;
-    TILE_END
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    double xw = B.x[c - g.sx], xc = B.x[c];
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double xe = B.x[c + g.sx];
+        double r = B.b[c] - apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, B.x, c);
+        B.r[c] = r;
+        B.r0[c] = r;
+        B.q[c] = 0;
+        acc += r * r;
+        xw = xc;
+        xc = xe;
+    }
+    SEGMENT_END
     if (seq) return;
     double vals[1] = {acc};
     if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) fin_init(st, vals[0]);
@@ -209,51 +251,56 @@ k_bicg_init(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int seq, Partials<1>
 // guess, which is exactly 0 + (p - 0)/ac (src/eq.h:367-368); with SOR
 // the zero guess itself (src/eq.h:438).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_p(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int first_sweep, const KrylovState *st) {
+k_bicg_p(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int first_sweep, const KrylovState *st) {
     if (st->done) return;
     const bool first = (st->it == 0);
     const double beta = st->beta, omega = st->omega;
-    TILE_LOOP(T)
-    double pv = first ? B.r[c] : B.r[c] + beta * (B.pk[c] - omega * B.q[c]);
-    B.pk[c] = pv;
-    if (first_sweep) {
-        Coef7 a = coef7(C, i, j, k);
-        B.pp[c] = 0.0 + (pv - 0.0) / a.ac;
-    } else {
-        B.pp[c] = 0.0;
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double pv = first ? B.r[c] : B.r[c] + beta * (B.pk[c] - omega * B.q[c]);
+        B.pk[c] = pv;
+        B.pp[c] = first_sweep ? 0.0 + (pv - 0.0) / diag(C, cc, i) : 0.0;
     }
-    TILE_END
+    SEGMENT_END
 }
 
 // s = r - alpha q (src/eq.h:373-377) with the same first-sweep fusion.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_s(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, int first_sweep, const KrylovState *st) {
+k_bicg_s(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int first_sweep, const KrylovState *st) {
     if (st->done) return;
     const double alpha = st->alpha;
-    TILE_LOOP(T)
-    double sv = B.r[c] - alpha * B.q[c];
-    B.s[c] = sv;
-    if (first_sweep) {
-        Coef7 a = coef7(C, i, j, k);
-        B.ss[c] = 0.0 + (sv - 0.0) / a.ac;
-    } else {
-        B.ss[c] = 0.0;
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double sv = B.r[c] - alpha * B.q[c];
+        B.s[c] = sv;
+        B.ss[c] = first_sweep ? 0.0 + (sv - 0.0) / diag(C, cc, i) : 0.0;
     }
-    TILE_END
+    SEGMENT_END
 }
 
 // q = A pp and <r0, q>; alpha = rho / <r0, q> (src/eq.h:369-371).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_q(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ppf, int seq,
+k_bicg_q(Grid g, PoissonCoef C, Segments S, PoissonBufs B, const double *ppf, int seq,
          Partials<1> part, KrylovState *st) {
     if (st->done) return;
     double acc = 0;
-    TILE_LOOP(T)
-    Coef7 a = coef7(C, i, j, k);
-    double qv = apply_a(g, a, ppf, c);
-    B.q[c] = qv;
-    acc += B.r0[c] * qv;
-    TILE_END
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    double xw = ppf[c - g.sx], xc = ppf[c];
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double xe = ppf[c + g.sx];
+        double qv = apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, ppf, c);
+        B.q[c] = qv;
+        acc += B.r0[c] * qv;
+        xw = xc;
+        xc = xe;
+    }
+    SEGMENT_END
     if (seq) return;
     double vals[1] = {acc};
     if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) fin_q(st, vals[0]);
@@ -261,17 +308,24 @@ k_bicg_q(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ppf, int 
 
 // t = A ss, <t, s>, <t, t>; omega = <t,s>/<t,t> (src/eq.h:381-383).
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_t(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ssf, int seq,
+k_bicg_t(Grid g, PoissonCoef C, Segments S, PoissonBufs B, const double *ssf, int seq,
          Partials<2> part, KrylovState *st) {
     if (st->done) return;
     double ts = 0, tt = 0;
-    TILE_LOOP(T)
-    Coef7 a = coef7(C, i, j, k);
-    double tv = apply_a(g, a, ssf, c);
-    B.t[c] = tv;
-    ts += tv * B.s[c];
-    tt += tv * tv;
-    TILE_END
+    SEGMENT_LOOP(S)
+    ColumnCoef cc = column_coef(C, j, k);
+    long long c = c0;
+    double xw = ssf[c - g.sx], xc = ssf[c];
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        double xe = ssf[c + g.sx];
+        double tv = apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, ssf, c);
+        B.t[c] = tv;
+        ts += tv * B.s[c];
+        tt += tv * tv;
+        xw = xc;
+        xc = xe;
+    }
+    SEGMENT_END
     if (seq) return;
     double vals[2] = {ts, tt};
     if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) fin_t(st, vals[0], vals[1]);
@@ -280,18 +334,21 @@ k_bicg_t(Grid g, PoissonCoef C, Tiling T, PoissonBufs B, const double *ssf, int 
 // x += alpha pp + omega ss; r = s - omega t (src/eq.h:385-395) with
 // <r0, r> and <r, r> for the finisher.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_xr(Grid g, Tiling T, PoissonBufs B, const double *ppf, const double *ssf, int seq,
+k_bicg_xr(Grid g, Segments S, PoissonBufs B, const double *ppf, const double *ssf, int seq,
           Partials<2> part, KrylovState *st) {
     if (st->done) return;
     const double alpha = st->alpha, omega = st->omega;
     double r0r = 0, rr = 0;
-    TILE_LOOP(T)
-    B.x[c] = B.x[c] + alpha * ppf[c] + omega * ssf[c];
-    double rv = B.s[c] - omega * B.t[c];
-    B.r[c] = rv;
-    r0r += B.r0[c] * rv;
-    rr += rv * rv;
-    TILE_END
+    SEGMENT_LOOP(S)
+    long long c = c0;
+    for (int i = i0; i < i1; i++, c += g.sx) {
+        B.x[c] = B.x[c] + alpha * ppf[c] + omega * ssf[c];
+        double rv = B.s[c] - omega * B.t[c];
+        B.r[c] = rv;
+        r0r += B.r0[c] * rv;
+        rr += rv * rv;
+    }
+    SEGMENT_END
     if (seq) return;
     double vals[2] = {r0r, rr};
     if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) fin_xr(st, vals[0], vals[1]);
@@ -310,6 +367,10 @@ void seq_launch(const LaunchCtx &L, const Grid &g, int site, const double *a0, c
 
 }  // namespace
 
+Segments poisson_segments(const Grid &g, int sm_count) {
+    return Segments::make(interior_box(g), sm_count * 8);
+}
+
 void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it, double tol,
                           double ncell) {
     L.pre(KK_POISSON_BEGIN);
@@ -320,15 +381,15 @@ void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it,
 void launch_sor_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                           const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
                           KrylovState *st) {
-    Tiling T = Tiling::make(interior_box(g));
+    const Segments &S = cfg.seg;
     for (int color = 0; color < 2; color++) {
         L.pre(KK_SOR_SWEEP);
-        k_sor_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.b, cfg.relax, color, st);
+        k_sor_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.x, B.b, cfg.relax, color, st);
         L.post(KK_SOR_SWEEP);
     }
     double *rs = cfg.reference_sums ? B.r : nullptr;
     L.pre(KK_RESIDUAL_NORM);
-    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, nullptr, B.b, rs, part, st);
+    k_residual_norm<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.x, nullptr, B.b, rs, part, st);
     L.post(KK_RESIDUAL_NORM);
     if (rs) seq_launch(L, g, SEQ_RESIDUAL, B.r, B.r, nullptr, nullptr, st);
 }
@@ -336,13 +397,13 @@ void launch_sor_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &
 void launch_jacobi_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                              const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
                              KrylovState *st) {
-    Tiling T = Tiling::make(interior_box(g));
+    const Segments &S = cfg.seg;
     L.pre(KK_JACOBI_SWEEP);
-    k_jacobi_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.tp, B.x, B.b, st);
+    k_jacobi_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.tp, B.x, B.b, st);
     L.post(KK_JACOBI_SWEEP);
     double *rs = cfg.reference_sums ? B.r : nullptr;
     L.pre(KK_RESIDUAL_NORM);
-    k_residual_norm<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B.x, B.tp, B.b, rs, part, st);
+    k_residual_norm<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.x, B.tp, B.b, rs, part, st);
     L.post(KK_RESIDUAL_NORM);
     if (rs) seq_launch(L, g, SEQ_RESIDUAL, B.r, B.r, nullptr, nullptr, st);
 }
@@ -350,9 +411,9 @@ void launch_jacobi_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoe
 void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                       const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
                       KrylovState *st) {
-    Tiling T = Tiling::make(interior_box(g));
+    const Segments &S = cfg.seg;
     L.pre(KK_BICG_INIT);
-    k_bicg_init<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, cfg.reference_sums, part, st);
+    k_bicg_init<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, cfg.reference_sums, part, st);
     L.post(KK_BICG_INIT);
     if (cfg.reference_sums) seq_launch(L, g, SEQ_INIT, B.r0, B.r, nullptr, nullptr, st);
 }
@@ -360,14 +421,15 @@ void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
 // Applies the preconditioner to `rhs` with the first sweep already done
 // into `x` (Jacobi) or `x` zeroed (SOR); returns the buffer holding M^-1 rhs.
 static double *precondition(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
-                            const Tiling &T, const PoissonConfig &cfg, double *x, double *tmp,
-                            const double *rhs, const KrylovState *st) {
+                            const PoissonConfig &cfg, double *x, double *tmp, const double *rhs,
+                            const KrylovState *st) {
+    const Segments &S = cfg.seg;
     if (cfg.pc == PC_SOR) {
         for (int n = 0; n < cfg.pc_sweeps; n++) {
             for (int color = 0; color < 2; color++) {
                 L.pre(KK_SOR_SWEEP);
-                k_sor_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, x, rhs, cfg.pc_relax,
-                                                                 color, st);
+                k_sor_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, x, rhs, cfg.pc_relax,
+                                                                color, st);
                 L.post(KK_SOR_SWEEP);
             }
         }
@@ -376,7 +438,7 @@ static double *precondition(const LaunchCtx &L, const Grid &g, const PoissonCoef
     double *cur = x, *nxt = tmp;
     for (int n = 1; n < cfg.pc_sweeps; n++) {
         L.pre(KK_JACOBI_SWEEP);
-        k_jacobi_sweep<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, nxt, cur, rhs, st);
+        k_jacobi_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, nxt, cur, rhs, st);
         L.post(KK_JACOBI_SWEEP);
         double *t = cur;
         cur = nxt;
@@ -388,28 +450,28 @@ static double *precondition(const LaunchCtx &L, const Grid &g, const PoissonCoef
 void launch_bicg_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                            const PoissonBufs &B, const PoissonConfig &cfg, Partials<2> part,
                            KrylovState *st) {
-    Tiling T = Tiling::make(interior_box(g));
+    const Segments &S = cfg.seg;
     int first = (cfg.pc == PC_JACOBI && cfg.pc_sweeps >= 1) ? 1 : 0;
     int seq = cfg.reference_sums;
     Partials<1> part1{part.buf, part.ticket};
     L.pre(KK_BICG_P);
-    k_bicg_p<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, first, st);
+    k_bicg_p<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
     L.post(KK_BICG_P);
-    double *ppf = precondition(L, g, C, T, cfg, B.pp, B.tp, B.pk, st);
+    double *ppf = precondition(L, g, C, cfg, B.pp, B.tp, B.pk, st);
     L.pre(KK_BICG_Q);
-    k_bicg_q<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ppf, seq, part1, st);
+    k_bicg_q<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, ppf, seq, part1, st);
     L.post(KK_BICG_Q);
     if (seq) seq_launch(L, g, SEQ_Q, B.r0, B.q, nullptr, nullptr, st);
     L.pre(KK_BICG_S);
-    k_bicg_s<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, first, st);
+    k_bicg_s<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
     L.post(KK_BICG_S);
-    double *ssf = precondition(L, g, C, T, cfg, B.ss, B.ts, B.s, st);
+    double *ssf = precondition(L, g, C, cfg, B.ss, B.ts, B.s, st);
     L.pre(KK_BICG_T);
-    k_bicg_t<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, C, T, B, ssf, seq, part, st);
+    k_bicg_t<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, ssf, seq, part, st);
     L.post(KK_BICG_T);
     if (seq) seq_launch(L, g, SEQ_T, B.t, B.s, B.t, B.t, st);
     L.pre(KK_BICG_XR);
-    k_bicg_xr<<<L.blocks, TILE_THREADS, 0, L.s>>>(g, T, B, ppf, ssf, seq, part, st);
+    k_bicg_xr<<<S.count, TILE_THREADS, 0, L.s>>>(g, S, B, ppf, ssf, seq, part, st);
     L.post(KK_BICG_XR);
     if (seq) seq_launch(L, g, SEQ_XR, B.r0, B.r, B.r, B.r, st);
 }

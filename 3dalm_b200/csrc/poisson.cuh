@@ -33,7 +33,11 @@ struct PoissonConfig {
     double relax, pc_relax;
     int pc_sweeps;
     int reference_sums;  // 1: global sums in the reference's serial order
+    Segments seg;        // column segments of the interior (one per block)
 };
+
+// The interior's column segments, sized to fill the GPU.
+Segments poisson_segments(const Grid &g, int sm_count);
 
 void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it, double tol,
                           double ncell);
