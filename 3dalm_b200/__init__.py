@@ -38,7 +38,8 @@ EXPORTS = (
     "dalm_get_field", "dalm_set_field", "dalm_set_inflow_profile", "dalm_set_turbine_params",
     "dalm_step", "dalm_run_stage", "dalm_advance_clock", "dalm_get_step_stats",
     "dalm_set_poisson", "dalm_get_counts", "dalm_get_turbines", "dalm_get_points",
-    "dalm_synchronize", "dalm_get_stream", "dalm_get_timings", "dalm_kernel_kinds", "dalm_get_kernel_timing",
+    "dalm_synchronize", "dalm_get_stream", "dalm_get_timings", "dalm_kernel_kinds",
+    "dalm_get_kernel_timing", "dalm_diagnostics_noalloc",
 )
 
 

@@ -30,6 +30,9 @@ struct CudaError : std::runtime_error {
     explicit CudaError(const std::string &m) : std::runtime_error(m) {}
 };
 
+// Sets the message returned by dalm_last_error(NULL).
+void set_last_error(const std::string &msg);
+
 struct Grid {
     int nx, ny, nz, gc;      // stored sizes (incl. guide cells) and guide cells
     long long sx, sy, off;   // element strides and row offset

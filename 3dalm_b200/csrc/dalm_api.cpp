@@ -35,6 +35,13 @@ const char *kKindNames[KK_COUNT] = {
     "bicg_init", "bicg_p", "bicg_q", "bicg_s", "bicg_t", "bicg_xr",
     "poisson_begin", "layout", "seq_sum"};
 
+}  // namespace
+
+// Message for dalm_last_error(NULL) from translation units without a handle.
+void dalm::set_last_error(const std::string &msg) { g_last_error = msg; }
+
+namespace {
+
 struct EventPair {
     cudaEvent_t a, b;
     int kind;

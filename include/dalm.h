@@ -211,6 +211,28 @@ int dalm_kernel_kinds(void);
 int dalm_get_kernel_timing(dalm_handle *h, int index, const char **name,
                            int64_t *launches, double *ms, double *bytes_per_launch);
 
+/* No counterpart in the reference (its diagnostics run inside its own
+ * OpenACC data region).  For callers that cannot let a library allocate
+ * device memory -- an OpenACC program that keeps U and JU in its own data
+ * region and passes device pointers via `host_data use_device`, a caller
+ * whose memory pool already owns the device, or code that must not
+ * allocate in the middle of a time step -- this computes the step
+ * diagnostics of a state already in device memory without any allocation:
+ * out[0] = ||div(JU)||_2 / sqrt(N) (calc_divergence + calc_l2_norm) and
+ * out[1] = max CFL (calc_max_cfl), written to the device array `out`.
+ * U and JU are device arrays in the reference layout ([len][3] with guide
+ * cells), dx, dy, dz device arrays of the stored lengths, stream a
+ * cudaStream_t (NULL: the default stream); the work is asynchronous.
+ * Limit: the reduction keeps one partial per 32 x 8 x 16 block of interior
+ * cells in a fixed 256 KiB device array, so at most 16384 such blocks
+ * (512 x 256 x 128 interior cells need 4096); larger grids return
+ * DALM_ERR_UNSUPPORTED.  The first call on a device looks up that array's
+ * address and must come before any stream capture; calls that overlap on
+ * the GPU share the array and race. */
+int dalm_diagnostics_noalloc(const double *U, const double *JU, const double *dx,
+                             const double *dy, const double *dz, const int64_t size[3],
+                             int64_t gc, double dt, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
