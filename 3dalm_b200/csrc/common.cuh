@@ -30,6 +30,11 @@ struct CudaError : std::runtime_error {
     explicit CudaError(const std::string &m) : std::runtime_error(m) {}
 };
 
+// A bounded device-side wait ran out (reported as DALM_ERR_DEVICE_WAIT).
+struct DeviceWaitError : std::runtime_error {
+    explicit DeviceWaitError(const std::string &m) : std::runtime_error(m) {}
+};
+
 // Sets the message returned by dalm_last_error(NULL).
 void set_last_error(const std::string &msg);
 

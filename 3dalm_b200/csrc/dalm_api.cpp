@@ -75,6 +75,7 @@ struct dalm_handle {
     double *staging = nullptr;   // reference-layout staging buffer (3*len)
     PoissonBufs pb{};
     PoissonConfig pcfg{};
+    MapTable maps;
     double *partial = nullptr;
     unsigned int *ticket = nullptr;
     KrylovState *d_kst = nullptr, *h_kst = nullptr;
@@ -250,6 +251,10 @@ struct dalm_handle {
         pcfg.pc_sweeps = (int)cs.pc_max_it;
         pcfg.reference_sums = opt.reference_sums ? 1 : 0;
         pcfg.seg = poisson_segments(g, sm_count);
+        const double *tma_fields[] = {pb.x, pb.b, pb.r, pb.r0, pb.pk, pb.q,
+                                      pb.s, pb.t, pb.pp, pb.ss, pb.tp, pb.ts};
+        for (const double *v : tma_fields) maps.add(g, v);
+        pcfg.maps = &maps;
         partial = dalloc<double>((size_t)std::max(L.blocks, pcfg.seg.count) * 4);
         ticket = dalloc<unsigned int>(1);
         d_kst = dalloc<KrylovState>(1);
@@ -425,6 +430,7 @@ struct dalm_handle {
             issued += batch;
             DALM_CUDA(cudaMemcpyAsync(h_kst, d_kst, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream));
             DALM_CUDA(cudaStreamSynchronize(stream));
+            if (h_kst->wait_error) throw DeviceWaitError("a TMA stage wait in the Poisson solver ran out");
             if (h_kst->done) break;
             if (issued > max_it + 1)
                 throw std::runtime_error("Poisson loop did not stop at its iteration limit");
@@ -650,6 +656,10 @@ struct dalm_handle {
     catch (const CudaError &e) {                       \
         (h)->err = e.what();                           \
         return DALM_ERR_CUDA;                          \
+    }                                                  \
+    catch (const DeviceWaitError &e) {                 \
+        (h)->err = e.what();                           \
+        return DALM_ERR_DEVICE_WAIT;                   \
     }                                                  \
     catch (const std::invalid_argument &e) {           \
         (h)->err = e.what();                           \

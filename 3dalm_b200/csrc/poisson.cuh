@@ -2,6 +2,7 @@
 #pragma once
 
 #include "flow.cuh"
+#include "tma.cuh"
 
 namespace dalm {
 
@@ -14,7 +15,7 @@ struct KrylovState {
     double tol;
     long long it, max_it;
     int done;         // 1 once the reference loop would have exited
-    int pad;
+    int wait_error;   // non-zero: a bounded device-side wait ran out
 };
 
 struct PoissonBufs {
@@ -23,6 +24,24 @@ struct PoissonBufs {
     double *r, *r0, *pk, *q, *s, *t;   // Eq::r, r0, p, q, s, t
     double *pp, *ss;       // preconditioned directions (Eq::pp, Eq::ss)
     double *tp, *ts;       // Jacobi ping-pong partners of pp and ss
+};
+
+// TMA maps of every Poisson buffer, looked up by device pointer.
+struct MapTable {
+    static constexpr int MAX = 16;
+    int n = 0;
+    const void *ptr[MAX];
+    FieldMaps maps[MAX];
+    void add(const Grid &g, const void *p) {
+        ptr[n] = p;
+        maps[n] = make_field_maps(g, p, 8);
+        n++;
+    }
+    const FieldMaps &of(const void *p) const {
+        for (int m = 0; m < n; m++)
+            if (ptr[m] == p) return maps[m];
+        throw std::invalid_argument("no TMA map for this buffer");
+    }
 };
 
 enum PoissonMethod { PM_SOR = 0, PM_BICG = 1, PM_JACOBI = 2 };
@@ -34,10 +53,13 @@ struct PoissonConfig {
     int pc_sweeps;
     int reference_sums;  // 1: global sums in the reference's serial order
     Segments seg;        // column segments of the interior (one per block)
+    const MapTable *maps;
 };
 
 // The interior's column segments, sized to fill the GPU.
 Segments poisson_segments(const Grid &g, int sm_count);
+// Dynamic shared memory of the TMA stencil kernels (one ring per block).
+size_t poisson_stencil_smem();
 
 void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it, double tol,
                           double ncell);

@@ -8,9 +8,11 @@
 // mode, serially in the reference's cell order (k_seq).
 //
 // Kernels walk column segments (Segments): a block owns 32 (k) x 8 (j)
-// cells of a column and marches through a chunk of i-planes, rotating the
-// west / centre / east values of the stencil operand through registers, so
-// each plane of the operand is read once from DRAM per sweep.
+// cells of a column and marches through a chunk of i-planes.  The stencil
+// kernels stage each plane of their operand (with a one-cell halo in j and
+// two in k) and of their point-wise input in shared memory with TMA
+// (cp.async.bulk.tensor), NSTAGE planes deep, so the loads of the next
+// planes are in flight while the current plane is computed.
 #include <cfloat>
 
 #include "poisson.cuh"
@@ -44,15 +46,6 @@ __device__ __forceinline__ double diag(const PoissonCoef &C, const ColumnCoef &c
     return acu / C.max_diag;
 }
 
-// ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb, left to right
-// (src/mv.h:87, 214; src/eq.h:36, 177); xw, xc, xe come from registers.
-__device__ __forceinline__ double apply_a(const Grid &g, double ac, double ae, double aw,
-                                          const ColumnCoef &cc, double xw, double xc, double xe,
-                                          const double *v, long long c) {
-    return ac * xc + ae * xe + aw * xw + cc.an * v[c + g.sy] + cc.as * v[c - g.sy] +
-           cc.at * v[c + 1] + cc.ab * v[c - 1];
-}
-
 #define SEGMENT_LOOP(S)                                                   \
     for (int u = blockIdx.x; u < (S).count; u += gridDim.x) {             \
         int i0, i1, j, k;                                                 \
@@ -63,7 +56,7 @@ __device__ __forceinline__ double apply_a(const Grid &g, double ac, double ae, d
 
 __global__ void k_begin(KrylovState *st, long long max_it, double tol, double ncell) {
     st->rho = 0; st->rho_old = 1; st->alpha = 1; st->omega = 1; st->beta = 0; st->err = 0;
-    st->ncell = ncell; st->tol = tol; st->it = 0; st->max_it = max_it; st->done = 0;
+    st->ncell = ncell; st->tol = tol; st->it = 0; st->max_it = max_it; st->done = 0; st->wait_error = 0;
 }
 
 // Residual norm at the end of a SOR / Jacobi iteration and the stop rule
@@ -72,81 +65,6 @@ __device__ __forceinline__ void finish_iteration(KrylovState *st, double sum_r2)
     st->err = sqrt(sum_r2) / sqrt(st->ncell);
     st->it += 1;
     if (!(st->it < st->max_it && st->err > st->tol)) st->done = 1;
-}
-
-// ---------------------------------------------------------------- SOR
-
-// sweep_sor_at_cell (src/eq.h:145-181), colour (i+j+k)%2 (offsets 0).
-// The colour's cells are updated in place; their neighbours all have the
-// other colour, so the registers rotated along i are never stale.
-__global__ void __launch_bounds__(TILE_THREADS)
-k_sor_sweep(Grid g, PoissonCoef C, Segments S, double *x, const double *b, double w, int color,
-            const KrylovState *st) {
-    if (st->done) return;
-    SEGMENT_LOOP(S)
-    ColumnCoef cc = column_coef(C, j, k);
-    long long c = c0;
-    double xw = x[c - g.sx], xc = x[c];
-    for (int i = i0; i < i1; i++, c += g.sx) {
-        double xe = x[c + g.sx];
-        if (((i + j + k) & 1) == color) {
-            double ac = diag(C, cc, i);
-            double rel = (b[c] - apply_a(g, ac, C.ae[i], C.aw[i], cc, xw, xc, xe, x, c)) / ac;
-            xc = xc + w * rel;
-            x[c] = xc;
-        }
-        xw = xc;
-        xc = xe;
-    }
-    SEGMENT_END
-}
-
-// calc_residual + calc_l2_norm (src/mv.h:33-182) fused; when `copy_from`
-// is set the iterate lives there (Jacobi ping-pong) and is copied into x.
-// With `rstore` the residual is stored (reference-order sums read it back).
-__global__ void __launch_bounds__(TILE_THREADS)
-k_residual_norm(Grid g, PoissonCoef C, Segments S, double *x, const double *copy_from,
-                const double *b, double *rstore, Partials<1> part, KrylovState *st) {
-    if (st->done) return;
-    const double *v = copy_from ? copy_from : x;
-    double acc = 0;
-    SEGMENT_LOOP(S)
-    ColumnCoef cc = column_coef(C, j, k);
-    long long c = c0;
-    double xw = v[c - g.sx], xc = v[c];
-    for (int i = i0; i < i1; i++, c += g.sx) {
-        double xe = v[c + g.sx];
-        double r = b[c] - apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, v, c);
-        acc += r * r;
-        if (rstore) rstore[c] = r;
-        if (copy_from) x[c] = xc;
-        xw = xc;
-        xc = xe;
-    }
-    SEGMENT_END
-    if (rstore) return;
-    double vals[1] = {acc};
-    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) finish_iteration(st, vals[0]);
-}
-
-// sweep_jacobi_at_cell (src/eq.h:6-39): out = in + (rhs - A in)/ac.
-__global__ void __launch_bounds__(TILE_THREADS)
-k_jacobi_sweep(Grid g, PoissonCoef C, Segments S, double *out, const double *in, const double *rhs,
-               const KrylovState *st) {
-    if (st->done) return;
-    SEGMENT_LOOP(S)
-    ColumnCoef cc = column_coef(C, j, k);
-    long long c = c0;
-    double xw = in[c - g.sx], xc = in[c];
-    for (int i = i0; i < i1; i++, c += g.sx) {
-        double xe = in[c + g.sx];
-        double ac = diag(C, cc, i);
-        double rel = (rhs[c] - apply_a(g, ac, C.ae[i], C.aw[i], cc, xw, xc, xe, in, c)) / ac;
-        out[c] = xc + rel;
-        xw = xc;
-        xc = xe;
-    }
-    SEGMENT_END
 }
 
 // ------------------------------------------------------------ BiCGStab
@@ -220,32 +138,6 @@ __global__ void k_seq(Grid g, int site, const double *a0, const double *b0, cons
     }
 }
 
-// calc_residual, cpy_array(r0, r), fill(q, 0) and the first rho = <r0, r>
-// (src/eq.h:342-353).
-__global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_init(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int seq, Partials<1> part,
-            KrylovState *st) {
-    double acc = 0;
-    SEGMENT_LOOP(S)
-    ColumnCoef cc = column_coef(C, j, k);
-    long long c = c0;
-    double xw = B.x[c - g.sx], xc = B.x[c];
-    for (int i = i0; i < i1; i++, c += g.sx) {
-        double xe = B.x[c + g.sx];
-        double r = B.b[c] - apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, B.x, c);
-        B.r[c] = r;
-        B.r0[c] = r;
-        B.q[c] = 0;
-        acc += r * r;
-        xw = xc;
-        xc = xe;
-    }
-    SEGMENT_END
-    if (seq) return;
-    double vals[1] = {acc};
-    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) fin_init(st, vals[0]);
-}
-
 // p = r (it 0) or r + beta (p - omega q) (src/eq.h:355-365); with the
 // Jacobi preconditioner also the first sweep of run_jacobi_pc from a zero
 // guess, which is exactly 0 + (p - 0)/ac (src/eq.h:367-368); with SOR
@@ -282,55 +174,6 @@ k_bicg_s(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int first_sweep, cons
     SEGMENT_END
 }
 
-// q = A pp and <r0, q>; alpha = rho / <r0, q> (src/eq.h:369-371).
-__global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_q(Grid g, PoissonCoef C, Segments S, PoissonBufs B, const double *ppf, int seq,
-         Partials<1> part, KrylovState *st) {
-    if (st->done) return;
-    double acc = 0;
-    SEGMENT_LOOP(S)
-    ColumnCoef cc = column_coef(C, j, k);
-    long long c = c0;
-    double xw = ppf[c - g.sx], xc = ppf[c];
-    for (int i = i0; i < i1; i++, c += g.sx) {
-        double xe = ppf[c + g.sx];
-        double qv = apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, ppf, c);
-        B.q[c] = qv;
-        acc += B.r0[c] * qv;
-        xw = xc;
-        xc = xe;
-    }
-    SEGMENT_END
-    if (seq) return;
-    double vals[1] = {acc};
-    if (grid_reduce<1>(vals, 0u, part) && threadIdx.x == 0) fin_q(st, vals[0]);
-}
-
-// t = A ss, <t, s>, <t, t>; omega = <t,s>/<t,t> (src/eq.h:381-383).
-__global__ void __launch_bounds__(TILE_THREADS)
-k_bicg_t(Grid g, PoissonCoef C, Segments S, PoissonBufs B, const double *ssf, int seq,
-         Partials<2> part, KrylovState *st) {
-    if (st->done) return;
-    double ts = 0, tt = 0;
-    SEGMENT_LOOP(S)
-    ColumnCoef cc = column_coef(C, j, k);
-    long long c = c0;
-    double xw = ssf[c - g.sx], xc = ssf[c];
-    for (int i = i0; i < i1; i++, c += g.sx) {
-        double xe = ssf[c + g.sx];
-        double tv = apply_a(g, diag(C, cc, i), C.ae[i], C.aw[i], cc, xw, xc, xe, ssf, c);
-        B.t[c] = tv;
-        ts += tv * B.s[c];
-        tt += tv * tv;
-        xw = xc;
-        xc = xe;
-    }
-    SEGMENT_END
-    if (seq) return;
-    double vals[2] = {ts, tt};
-    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) fin_t(st, vals[0], vals[1]);
-}
-
 // x += alpha pp + omega ss; r = s - omega t (src/eq.h:385-395) with
 // <r0, r> and <r, r> for the finisher.
 __global__ void __launch_bounds__(TILE_THREADS)
@@ -354,6 +197,150 @@ k_bicg_xr(Grid g, Segments S, PoissonBufs B, const double *ppf, const double *ss
     if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) fin_xr(st, vals[0], vals[1]);
 }
 
+
+// ------------------------------------------------------- TMA stencil sweeps
+
+constexpr int NSTAGE = 6;
+constexpr int HK = 2;                         // halo in k: 16 bytes of FP64
+constexpr int TKW = TK + 2 * HK;              // 36
+constexpr int TJW = TJ + 2;                   // 10
+constexpr int OP_ELEMS = TKW * TJW;
+constexpr int OP_BYTES = OP_ELEMS * 8;        // 2880
+constexpr int OP_BYTES_PAD = ((OP_BYTES + 127) / 128) * 128;
+constexpr int PW_BYTES = TK * TJ * 8;         // 2048
+constexpr int STAGE_BYTES = OP_BYTES_PAD + PW_BYTES;
+
+enum StencilKind {
+    SK_JACOBI = 0,    // out = x + (rhs - A x)/ac          sweep_jacobi_at_cell, src/eq.h:6-39
+    SK_RESIDUAL = 1,  // sum (b - A x)^2 [, r stored] [, x copied]   src/mv.h:33-182
+    SK_INIT = 2,      // r = r0 = b - A x, q = 0, sum r*r         src/eq.h:342-353
+    SK_Q = 3,         // q = A pp, sum r0*q                       src/eq.h:369-371
+    SK_T = 4,         // t = A ss, sum t*s, sum t*t               src/eq.h:381-383
+    SK_SOR = 5        // red-black update in place                src/eq.h:145-181
+};
+
+struct StencilArgs {
+    double *out;    // JACOBI out, RESIDUAL r (or null), INIT r, Q q, T t, SOR x
+    double *out2;   // RESIDUAL copy target (or null), INIT r0
+    double *out3;   // INIT q
+    double w;       // SOR relaxation
+    int color;      // SOR colour
+    int reduce;     // 0: no tree reduction (the reference-order path sums)
+};
+
+// One block = one column segment.  Load L (0 <= L < nplanes + 2) brings
+// plane i0 - 1 + L of the operand (halo box) and, for the planes the block
+// computes, of the point-wise input (plain box) into ring stage L % NSTAGE.
+// Plane i0 + n is computed from loads n, n + 1, n + 2; after it, its stage
+// (load n) is refilled with load n + NSTAGE.
+template <int KIND>
+__global__ void __launch_bounds__(TILE_THREADS)
+k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m_op,
+          const __grid_constant__ CUtensorMap m_pw, StencilArgs A, Partials<2> part,
+          KrylovState *st) {
+    if (KIND != SK_INIT && st->done) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long bar[NSTAGE];
+    const int u = blockIdx.x;
+    int i0, i1, j, k;
+    const bool active = S.column(u, i0, i1, j, k);
+    const int col = u % S.ncol;
+    const int k0 = S.box.lo[2] + (col % S.ntk) * TK, j0 = S.box.lo[1] + (col / S.ntk) * TJ;
+    const int nplanes = i1 - i0, nload = nplanes + 2;
+    const int xo = k0 - HK + (int)g.off, xp = k0 + (int)g.off;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSTAGE; s++) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](int L) {
+        int s = L % NSTAGE;
+        unsigned char *base = smem + s * STAGE_BYTES;
+        bool pw = (L >= 1 && L <= nplanes);
+        mbar_expect_tx(&bar[s], OP_BYTES + (pw ? PW_BYTES : 0));
+        tma_load_3d(base, &m_op, xo, j0 - 1, i0 - 1 + L, &bar[s]);
+        if (pw) tma_load_3d(base + OP_BYTES_PAD, &m_pw, xp, j0, i0 - 1 + L, &bar[s]);
+    };
+    int issued = 0;
+    if (threadIdx.x == 0)
+        for (; issued < NSTAGE && issued < nload; issued++) issue(issued);
+
+    ColumnCoef cc;
+    if (active) cc = column_coef(C, j, k);
+    const int idx = (warp + 1) * TKW + lane + HK;
+    double acc0 = 0, acc1 = 0;
+    int waited = 0;
+    bool fail = false;
+    for (int n = 0; n < nplanes; n++) {
+        while (!fail && waited <= n + 2) {
+            fail = !mbar_wait(&bar[waited % NSTAGE], (unsigned)((waited / NSTAGE) & 1));
+            if (!fail) waited++;
+        }
+        if (!fail && active) {
+            const double *W = (const double *)(smem + (n % NSTAGE) * STAGE_BYTES);
+            const double *Cp = (const double *)(smem + ((n + 1) % NSTAGE) * STAGE_BYTES);
+            const double *E = (const double *)(smem + ((n + 2) % NSTAGE) * STAGE_BYTES);
+            const double pw = ((const double *)((const unsigned char *)Cp + OP_BYTES_PAD))[warp * TK + lane];
+            const int i = i0 + n;
+            const long long c = g.at(i, j, k);
+            const double xc = Cp[idx];
+            const double ac = diag(C, cc, i);
+            // ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb, left to right
+            const double ax = ac * xc + C.ae[i] * E[idx] + C.aw[i] * W[idx] + cc.an * Cp[idx + TKW] +
+                              cc.as * Cp[idx - TKW] + cc.at * Cp[idx + 1] + cc.ab * Cp[idx - 1];
+            if (KIND == SK_JACOBI) {
+                A.out[c] = xc + (pw - ax) / ac;
+            } else if (KIND == SK_RESIDUAL) {
+                double r = pw - ax;
+                acc0 += r * r;
+                if (A.out) A.out[c] = r;
+                if (A.out2) A.out2[c] = xc;
+            } else if (KIND == SK_INIT) {
+                double r = pw - ax;
+                A.out[c] = r;
+                A.out2[c] = r;
+                A.out3[c] = 0;
+                acc0 += r * r;
+            } else if (KIND == SK_Q) {
+                A.out[c] = ax;
+                acc0 += pw * ax;
+            } else if (KIND == SK_T) {
+                A.out[c] = ax;
+                acc0 += ax * pw;
+                acc1 += ax * ax;
+            } else if (KIND == SK_SOR) {
+                if (((i + j + k) & 1) == A.color) A.out[c] = xc + A.w * ((pw - ax) / ac);
+            }
+        }
+        if (__syncthreads_or(fail)) break;
+        if (threadIdx.x == 0 && issued < nload) {
+            fence_proxy_async();  // stage n was read through the generic proxy
+            issue(issued);
+            issued++;
+        }
+    }
+    if (__syncthreads_or(fail)) {
+        // a bounded wait ran out: report, drain what is still in flight, stop
+        if (threadIdx.x == 0) {
+            st->wait_error = 1;
+            st->done = 1;
+            for (int L = waited; L < issued; L++)
+                mbar_wait(&bar[L % NSTAGE], (unsigned)((L / NSTAGE) & 1));
+        }
+        return;
+    }
+    if (KIND == SK_JACOBI || KIND == SK_SOR || !A.reduce) return;
+    double vals[2] = {acc0, acc1};
+    if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) {
+        if (KIND == SK_RESIDUAL) finish_iteration(st, vals[0]);
+        if (KIND == SK_INIT) fin_init(st, vals[0]);
+        if (KIND == SK_Q) fin_q(st, vals[0]);
+        if (KIND == SK_T) fin_t(st, vals[0], vals[1]);
+    }
+}
+
 Box interior_box(const Grid &g) {
     return Box{{g.gc, g.gc, g.gc}, {g.nx - g.gc, g.ny - g.gc, g.nz - g.gc}};
 }
@@ -365,11 +352,24 @@ void seq_launch(const LaunchCtx &L, const Grid &g, int site, const double *a0, c
     L.post(KK_SEQ_SUM);
 }
 
+template <int KIND>
+void stencil_launch(const LaunchCtx &L, int kind_tag, const Grid &g, const PoissonCoef &C,
+                    const PoissonConfig &cfg, const double *op, const double *pw,
+                    const StencilArgs &A, Partials<2> part, KrylovState *st) {
+    const Segments &S = cfg.seg;
+    L.pre(kind_tag);
+    k_stencil<KIND><<<S.count, TILE_THREADS, NSTAGE * STAGE_BYTES, L.s>>>(
+        g, C, S, cfg.maps->of(op).halo, cfg.maps->of(pw).plain, A, part, st);
+    L.post(kind_tag);
+}
+
 }  // namespace
 
 Segments poisson_segments(const Grid &g, int sm_count) {
     return Segments::make(interior_box(g), sm_count * 8);
 }
+
+size_t poisson_stencil_smem() { return (size_t)NSTAGE * STAGE_BYTES; }
 
 void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it, double tol,
                           double ncell) {
@@ -378,43 +378,50 @@ void launch_poisson_begin(const LaunchCtx &L, KrylovState *st, long long max_it,
     L.post(KK_POISSON_BEGIN);
 }
 
+static void sor_sweep(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                      const PoissonConfig &cfg, double *x, const double *rhs, double w, int color,
+                      KrylovState *st) {
+    StencilArgs A{x, nullptr, nullptr, w, color, 0};
+    stencil_launch<SK_SOR>(L, KK_SOR_SWEEP, g, C, cfg, x, rhs, A, Partials<2>{nullptr, nullptr}, st);
+}
+
+static void jacobi_sweep(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
+                         const PoissonConfig &cfg, double *out, const double *in,
+                         const double *rhs, KrylovState *st) {
+    StencilArgs A{out, nullptr, nullptr, 0, 0, 0};
+    stencil_launch<SK_JACOBI>(L, KK_JACOBI_SWEEP, g, C, cfg, in, rhs, A,
+                              Partials<2>{nullptr, nullptr}, st);
+}
+
 void launch_sor_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                           const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
                           KrylovState *st) {
-    const Segments &S = cfg.seg;
-    for (int color = 0; color < 2; color++) {
-        L.pre(KK_SOR_SWEEP);
-        k_sor_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.x, B.b, cfg.relax, color, st);
-        L.post(KK_SOR_SWEEP);
-    }
+    for (int color = 0; color < 2; color++)
+        sor_sweep(L, g, C, cfg, B.x, B.b, cfg.relax, color, st);
     double *rs = cfg.reference_sums ? B.r : nullptr;
-    L.pre(KK_RESIDUAL_NORM);
-    k_residual_norm<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.x, nullptr, B.b, rs, part, st);
-    L.post(KK_RESIDUAL_NORM);
+    StencilArgs A{rs, nullptr, nullptr, 0, 0, !cfg.reference_sums};
+    stencil_launch<SK_RESIDUAL>(L, KK_RESIDUAL_NORM, g, C, cfg, B.x, B.b, A,
+                                Partials<2>{part.buf, part.ticket}, st);
     if (rs) seq_launch(L, g, SEQ_RESIDUAL, B.r, B.r, nullptr, nullptr, st);
 }
 
 void launch_jacobi_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                              const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
                              KrylovState *st) {
-    const Segments &S = cfg.seg;
-    L.pre(KK_JACOBI_SWEEP);
-    k_jacobi_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.tp, B.x, B.b, st);
-    L.post(KK_JACOBI_SWEEP);
+    jacobi_sweep(L, g, C, cfg, B.tp, B.x, B.b, st);
     double *rs = cfg.reference_sums ? B.r : nullptr;
-    L.pre(KK_RESIDUAL_NORM);
-    k_residual_norm<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B.x, B.tp, B.b, rs, part, st);
-    L.post(KK_RESIDUAL_NORM);
+    StencilArgs A{rs, B.x, nullptr, 0, 0, !cfg.reference_sums};
+    stencil_launch<SK_RESIDUAL>(L, KK_RESIDUAL_NORM, g, C, cfg, B.tp, B.b, A,
+                                Partials<2>{part.buf, part.ticket}, st);
     if (rs) seq_launch(L, g, SEQ_RESIDUAL, B.r, B.r, nullptr, nullptr, st);
 }
 
 void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                       const PoissonBufs &B, const PoissonConfig &cfg, Partials<1> part,
                       KrylovState *st) {
-    const Segments &S = cfg.seg;
-    L.pre(KK_BICG_INIT);
-    k_bicg_init<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, cfg.reference_sums, part, st);
-    L.post(KK_BICG_INIT);
+    StencilArgs A{B.r, B.r0, B.q, 0, 0, !cfg.reference_sums};
+    stencil_launch<SK_INIT>(L, KK_BICG_INIT, g, C, cfg, B.x, B.b, A,
+                            Partials<2>{part.buf, part.ticket}, st);
     if (cfg.reference_sums) seq_launch(L, g, SEQ_INIT, B.r0, B.r, nullptr, nullptr, st);
 }
 
@@ -422,24 +429,16 @@ void launch_bicg_init(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
 // into `x` (Jacobi) or `x` zeroed (SOR); returns the buffer holding M^-1 rhs.
 static double *precondition(const LaunchCtx &L, const Grid &g, const PoissonCoef &C,
                             const PoissonConfig &cfg, double *x, double *tmp, const double *rhs,
-                            const KrylovState *st) {
-    const Segments &S = cfg.seg;
+                            KrylovState *st) {
     if (cfg.pc == PC_SOR) {
-        for (int n = 0; n < cfg.pc_sweeps; n++) {
-            for (int color = 0; color < 2; color++) {
-                L.pre(KK_SOR_SWEEP);
-                k_sor_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, x, rhs, cfg.pc_relax,
-                                                                color, st);
-                L.post(KK_SOR_SWEEP);
-            }
-        }
+        for (int n = 0; n < cfg.pc_sweeps; n++)
+            for (int color = 0; color < 2; color++)
+                sor_sweep(L, g, C, cfg, x, rhs, cfg.pc_relax, color, st);
         return x;
     }
     double *cur = x, *nxt = tmp;
     for (int n = 1; n < cfg.pc_sweeps; n++) {
-        L.pre(KK_JACOBI_SWEEP);
-        k_jacobi_sweep<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, nxt, cur, rhs, st);
-        L.post(KK_JACOBI_SWEEP);
+        jacobi_sweep(L, g, C, cfg, nxt, cur, rhs, st);
         double *t = cur;
         cur = nxt;
         nxt = t;
@@ -453,22 +452,19 @@ void launch_bicg_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef 
     const Segments &S = cfg.seg;
     int first = (cfg.pc == PC_JACOBI && cfg.pc_sweeps >= 1) ? 1 : 0;
     int seq = cfg.reference_sums;
-    Partials<1> part1{part.buf, part.ticket};
     L.pre(KK_BICG_P);
     k_bicg_p<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
     L.post(KK_BICG_P);
     double *ppf = precondition(L, g, C, cfg, B.pp, B.tp, B.pk, st);
-    L.pre(KK_BICG_Q);
-    k_bicg_q<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, ppf, seq, part1, st);
-    L.post(KK_BICG_Q);
+    StencilArgs Aq{B.q, nullptr, nullptr, 0, 0, !seq};
+    stencil_launch<SK_Q>(L, KK_BICG_Q, g, C, cfg, ppf, B.r0, Aq, part, st);
     if (seq) seq_launch(L, g, SEQ_Q, B.r0, B.q, nullptr, nullptr, st);
     L.pre(KK_BICG_S);
     k_bicg_s<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
     L.post(KK_BICG_S);
     double *ssf = precondition(L, g, C, cfg, B.ss, B.ts, B.s, st);
-    L.pre(KK_BICG_T);
-    k_bicg_t<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, ssf, seq, part, st);
-    L.post(KK_BICG_T);
+    StencilArgs At{B.t, nullptr, nullptr, 0, 0, !seq};
+    stencil_launch<SK_T>(L, KK_BICG_T, g, C, cfg, ssf, B.s, At, part, st);
     if (seq) seq_launch(L, g, SEQ_T, B.t, B.s, B.t, B.t, st);
     L.pre(KK_BICG_XR);
     k_bicg_xr<<<S.count, TILE_THREADS, 0, L.s>>>(g, S, B, ppf, ssf, seq, part, st);
