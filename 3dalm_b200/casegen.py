@@ -354,3 +354,47 @@ def config(name: str, **over) -> CaseSpec:
     for k, v in over.items():
         setattr(spec, k, v)
     return spec
+
+
+STATE_FILE = "initial_U.f64"       # U[NX][NY][NZ][3] float64, guide cells included
+PROFILE_FILE = "inflow_profile.f64"  # [NY][NZ][3] float64 inflow ghost values
+
+
+def write_state_files(spec: CaseSpec, mesh: Mesh, case_dir: str) -> None:
+    """Raw little-endian float64 files the `dalm` command-line driver loads
+    when present: the seeded initial velocity and, for log-law cases, the
+    inflow profile."""
+    initial_velocity(spec, mesh).astype("<f8").tofile(os.path.join(case_dir, STATE_FILE))
+    prof = inflow_profile(spec, mesh)
+    if prof is not None:
+        prof.astype("<f8").tofile(os.path.join(case_dir, PROFILE_FILE))
+
+
+def main(argv=None):
+    import argparse
+
+    ap = argparse.ArgumentParser(description="write a 3dalm case directory")
+    ap.add_argument("config", help="c1..c5 or tiny-*")
+    ap.add_argument("case_dir")
+    ap.add_argument("--n", type=int, nargs=3, help="interior cells nx ny nz")
+    ap.add_argument("--steps", type=int, help="runtime.time = steps * dt")
+    ap.add_argument("--max-it", type=int, help="eq.\"max iteration\"")
+    ap.add_argument("--tol", type=float, help="eq.\"tolerance\"")
+    ap.add_argument("--seed", type=int)
+    ap.add_argument("--no-state", action="store_true", help="skip the initial-state files")
+    a = ap.parse_args(argv)
+    over = {}
+    if a.n:
+        over["n"] = tuple(a.n)
+    for key, val in (("steps", a.steps), ("max_it", a.max_it), ("tol", a.tol), ("seed", a.seed)):
+        if val is not None:
+            over[key] = val
+    spec = config(a.config, **over)
+    mesh = write_case(spec, a.case_dir)
+    if not a.no_state:
+        write_state_files(spec, mesh, a.case_dir)
+    print(a.case_dir)
+
+
+if __name__ == "__main__":
+    main()

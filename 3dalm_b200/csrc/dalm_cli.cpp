@@ -9,7 +9,22 @@
 #include <ctime>
 #include <vector>
 
+#include <string>
+
 #include "../../include/dalm.h"
+
+// Reads exactly v.size() doubles; false when the file is absent.
+static bool read_raw(const std::string &path, std::vector<double> &v) {
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    size_t n = fread(v.data(), sizeof(double), v.size(), f);
+    fclose(f);
+    if (n != v.size()) {
+        fprintf(stderr, "%s: expected %zu doubles, read %zu\n", path.c_str(), v.size(), n);
+        exit(1);
+    }
+    return true;
+}
 
 int main(int argc, char **argv) {
     if (argc < 2) {
@@ -33,6 +48,28 @@ int main(int argc, char **argv) {
         fprintf(stderr, "dalm_create failed (%d): %s\n", rc, dalm_last_error(nullptr));
         return 1;
     }
+    // Optional initial state written by the case generator (casegen.py):
+    // inflow_profile.f64 ([NY][NZ][3]) and initial_U.f64 ([NX][NY][NZ][3]),
+    // raw little-endian float64.  The reference always starts from uniform Uin.
+    int64_t size[3], gc;
+    dalm_get_size(h, size, &gc);
+    size_t cells = (size_t)(size[0] * size[1] * size[2]);
+    std::vector<double> prof((size_t)(size[1] * size[2] * 3)), U(cells * 3);
+    if (read_raw(std::string(dir) + "/inflow_profile.f64", prof)) {
+        if (dalm_set_inflow_profile(h, prof.data()) != DALM_OK) {
+            fprintf(stderr, "dalm_set_inflow_profile: %s\n", dalm_last_error(h));
+            return 1;
+        }
+    }
+    if (read_raw(std::string(dir) + "/initial_U.f64", U)) {
+        if (dalm_set_state(h, U.data(), nullptr, nullptr,
+                           DALM_SET_APPLY_UBC | DALM_SET_RECOMPUTE_JU) != DALM_OK) {
+            fprintf(stderr, "dalm_set_state: %s\n", dalm_last_error(h));
+            return 1;
+        }
+    }
+    U.clear();
+    U.shrink_to_fit();
     double dt = 0;
     int64_t max_step = 0;
     dalm_get_runtime(h, &dt, &max_step);
