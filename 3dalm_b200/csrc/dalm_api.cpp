@@ -336,6 +336,7 @@ struct dalm_handle {
         coef.an = upload(an); coef.as = upload(as);
         coef.at = upload(at); coef.ab = upload(ab);
         coef.max_diag = md;
+        coef.inv_max_diag = 1.0 / md;
         std::vector<double> xpart(NX, 0);
         for (int64_t i = 0; i < NX; i++) xpart[i] = (0.0 - ex[i]) - awu[i];
         coef.xpart = upload(xpart);

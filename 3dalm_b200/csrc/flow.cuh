@@ -27,6 +27,7 @@ struct PoissonCoef {
     const double *ae, *aw, *an, *as, *at, *ab;
     const double *xpart;  // (0 - ex[i]) - aw_u[i]: the first two steps of a_c
     double max_diag;
+    double inv_max_diag;  // 1 / max_diag (fast variant)
 };
 
 struct StepParams {

@@ -1,18 +1,23 @@
 // Pressure Poisson solvers (src/eq.h, src/mv.h) with matrix-free
 // coefficients and on-device loop control.
 //
-// Compiled with --fmad=false: each cell update keeps the reference's
-// operation order, so red-black SOR sweeps and Jacobi sweeps reproduce the
-// reference bit for bit.  Global dot products and norms are summed either
-// by a deterministic parallel tree (default) or, in reference-order-sum
-// mode, serially in the reference's cell order (k_seq).
+// Two arithmetic variants of every kernel (template flag EXACT):
+//   EXACT = true   the reference's operation order and rounding: separate
+//                  multiplies and adds (this file is compiled with
+//                  --fmad=false), true divisions by a_c.  Used together with
+//                  reference-order sums, the solve reproduces the reference
+//                  bit for bit.
+//   EXACT = false  fused multiply-adds and a Newton-refined reciprocal of a_c
+//                  (the fast default); results differ from the reference in
+//                  the last bits, like any other summation order.
 //
 // Kernels walk column segments (Segments): a block owns 32 (k) x 8 (j)
 // cells of a column and marches through a chunk of i-planes.  The stencil
-// kernels stage each plane of their operand (with a one-cell halo in j and
-// two in k) and of their point-wise input in shared memory with TMA
-// (cp.async.bulk.tensor), NSTAGE planes deep, so the loads of the next
-// planes are in flight while the current plane is computed.
+// kernels stage each plane of their operand (one-cell halo in j, two in k)
+// and of their point-wise input in shared memory with TMA
+// (cp.async.bulk.tensor), NSTAGE planes deep, and compute two planes per
+// pass, so the loads of the next planes are in flight while the current
+// ones are computed.
 #include <cfloat>
 
 #include "poisson.cuh"
@@ -21,29 +26,70 @@ namespace dalm {
 
 namespace {
 
-// Per-thread (fixed j, k) part of the coefficients: everything except the
-// i-dependent terms, hoisted out of the i march.
+// Per-thread (fixed j, k) part of the coefficients, hoisted out of the march.
 struct ColumnCoef {
     double an, as, at, ab;          // scaled (A[id][3..6] of the reference)
     double an_u, as_u, at_u, ab_u;  // unscaled, for the diagonal
+    double colsum;                  // an_u + as_u + at_u + ab_u (fast variant)
 };
 
 __device__ __forceinline__ ColumnCoef column_coef(const PoissonCoef &C, int j, int k) {
     ColumnCoef cc;
     cc.an = C.an[j]; cc.as = C.as[j]; cc.at = C.at[k]; cc.ab = C.ab[k];
     cc.an_u = C.an_u[j]; cc.as_u = C.as_u[j]; cc.at_u = C.at_u[k]; cc.ab_u = C.ab_u[k];
+    cc.colsum = cc.an_u + cc.as_u + cc.at_u + cc.ab_u;
     return cc;
 }
 
-// a_c of cell (i, j, k) exactly as build_A assembles and scales it
-// (src/eq.h:720-794): ((((((0 - ex) - aw) - an) - as) - at) - ab) / max_diag,
-// the first two subtractions precomputed per i in C.xpart.
-__device__ __forceinline__ double diag(const PoissonCoef &C, const ColumnCoef &cc, int i) {
-    double acu = C.xpart[i] - cc.an_u;
-    acu = acu - cc.as_u;
-    acu = acu - cc.at_u;
-    acu = acu - cc.ab_u;
-    return acu / C.max_diag;
+// a_c exactly as build_A assembles and scales it (src/eq.h:720-794):
+// ((((((0 - ex) - aw) - an) - as) - at) - ab) / max_diag, the first two
+// subtractions precomputed per i in xpart.
+template <bool EXACT>
+__device__ __forceinline__ double diag(double xpart, const ColumnCoef &cc, const PoissonCoef &C) {
+    if (EXACT) {
+        double acu = xpart - cc.an_u;
+        acu = acu - cc.as_u;
+        acu = acu - cc.at_u;
+        acu = acu - cc.ab_u;
+        return acu / C.max_diag;
+    }
+    return (xpart - cc.colsum) * C.inv_max_diag;
+}
+
+// 1/a with a Newton-Raphson refinement (two steps, quadratic convergence)
+// of the hardware's approximate reciprocal; a is a diagonal entry, never
+// near zero or subnormal.
+__device__ __forceinline__ double fast_rcp(double a) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+    double e = __fma_rn(-a, y, 1.0);
+    y = __fma_rn(y, e, y);
+    e = __fma_rn(-a, y, 1.0);
+    return __fma_rn(y, e, y);
+}
+
+// A x at one cell: ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb,
+// left to right (src/mv.h:87, 214; src/eq.h:36, 177).
+template <bool EXACT>
+__device__ __forceinline__ double apply_a(double ac, double ae, double aw, const ColumnCoef &cc,
+                                          double xc, double xe, double xw, double xn, double xs,
+                                          double xt, double xb) {
+    if (EXACT)
+        return ac * xc + ae * xe + aw * xw + cc.an * xn + cc.as * xs + cc.at * xt + cc.ab * xb;
+    double v = ac * xc;
+    v = __fma_rn(ae, xe, v);
+    v = __fma_rn(aw, xw, v);
+    v = __fma_rn(cc.an, xn, v);
+    v = __fma_rn(cc.as, xs, v);
+    v = __fma_rn(cc.at, xt, v);
+    return __fma_rn(cc.ab, xb, v);
+}
+
+// (b - ax)/ac, the Jacobi / SOR relaxation (src/eq.h:36, 177)
+template <bool EXACT>
+__device__ __forceinline__ double relax(double b, double ax, double ac) {
+    if (EXACT) return (b - ax) / ac;
+    return (b - ax) * fast_rcp(ac);
 }
 
 #define SEGMENT_LOOP(S)                                                   \
@@ -56,28 +102,19 @@ __device__ __forceinline__ double diag(const PoissonCoef &C, const ColumnCoef &c
 
 __global__ void k_begin(KrylovState *st, long long max_it, double tol, double ncell) {
     st->rho = 0; st->rho_old = 1; st->alpha = 1; st->omega = 1; st->beta = 0; st->err = 0;
-    st->ncell = ncell; st->tol = tol; st->it = 0; st->max_it = max_it; st->done = 0; st->wait_error = 0;
+    st->ncell = ncell; st->tol = tol; st->it = 0; st->max_it = max_it; st->done = 0;
+    st->wait_error = 0;
 }
 
-// Residual norm at the end of a SOR / Jacobi iteration and the stop rule
-// `while (it < max_it && err > tol)` (src/eq.h:297-305).
+// ---- finishers: the scalar updates after each global sum -----------------
+
+// residual norm of a SOR / Jacobi iteration and the stop rule
+// `while (it < max_it && err > tol)` (src/eq.h:297-305)
 __device__ __forceinline__ void finish_iteration(KrylovState *st, double sum_r2) {
     st->err = sqrt(sum_r2) / sqrt(st->ncell);
     st->it += 1;
     if (!(st->it < st->max_it && st->err > st->tol)) st->done = 1;
 }
-
-// ------------------------------------------------------------ BiCGStab
-//
-// run_pbicgstab (src/eq.h:333-473).  One iteration is
-//   p-update (+ first Jacobi sweep from zero) -> PC sweeps -> q = A pp, <r0,q>
-//   -> s-update (+ first sweep) -> PC sweeps -> t = A ss, <t,s>, <t,t>
-//   -> x, r update, <r0,r>, <r,r>
-// Each reduction's last block computes the next scalar (alpha, omega, err,
-// rho, beta) on the device.
-
-// ---- finishers: the scalar updates after each global sum -----------------
-
 // rho = <r0, r> and the breakdown test (src/eq.h:349-353)
 __device__ __forceinline__ void fin_init(KrylovState *st, double r0r) {
     st->rho = r0r;
@@ -138,10 +175,20 @@ __global__ void k_seq(Grid g, int site, const double *a0, const double *b0, cons
     }
 }
 
+// ---- point-wise BiCGStab kernels -------------------------------------------
+//
+// run_pbicgstab (src/eq.h:333-473).  One iteration is
+//   p-update (+ first Jacobi sweep from zero) -> PC sweeps -> q = A pp, <r0,q>
+//   -> s-update (+ first sweep) -> PC sweeps -> t = A ss, <t,s>, <t,t>
+//   -> x, r update, <r0,r>, <r,r>
+// Each reduction's last block computes the next scalar (alpha, omega, err,
+// rho, beta) on the device.
+
 // p = r (it 0) or r + beta (p - omega q) (src/eq.h:355-365); with the
 // Jacobi preconditioner also the first sweep of run_jacobi_pc from a zero
 // guess, which is exactly 0 + (p - 0)/ac (src/eq.h:367-368); with SOR
 // the zero guess itself (src/eq.h:438).
+template <bool EXACT>
 __global__ void __launch_bounds__(TILE_THREADS)
 k_bicg_p(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int first_sweep, const KrylovState *st) {
     if (st->done) return;
@@ -151,14 +198,22 @@ k_bicg_p(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int first_sweep, cons
     ColumnCoef cc = column_coef(C, j, k);
     long long c = c0;
     for (int i = i0; i < i1; i++, c += g.sx) {
-        double pv = first ? B.r[c] : B.r[c] + beta * (B.pk[c] - omega * B.q[c]);
+        double pv = first ? B.r[c]
+                          : (EXACT ? B.r[c] + beta * (B.pk[c] - omega * B.q[c])
+                                   : __fma_rn(beta, __fma_rn(-omega, B.q[c], B.pk[c]), B.r[c]));
         B.pk[c] = pv;
-        B.pp[c] = first_sweep ? 0.0 + (pv - 0.0) / diag(C, cc, i) : 0.0;
+        if (!first_sweep) {
+            B.pp[c] = 0.0;
+        } else {
+            double ac = diag<EXACT>(C.xpart[i], cc, C);
+            B.pp[c] = EXACT ? 0.0 + (pv - 0.0) / ac : pv * fast_rcp(ac);
+        }
     }
     SEGMENT_END
 }
 
 // s = r - alpha q (src/eq.h:373-377) with the same first-sweep fusion.
+template <bool EXACT>
 __global__ void __launch_bounds__(TILE_THREADS)
 k_bicg_s(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int first_sweep, const KrylovState *st) {
     if (st->done) return;
@@ -167,15 +222,21 @@ k_bicg_s(Grid g, PoissonCoef C, Segments S, PoissonBufs B, int first_sweep, cons
     ColumnCoef cc = column_coef(C, j, k);
     long long c = c0;
     for (int i = i0; i < i1; i++, c += g.sx) {
-        double sv = B.r[c] - alpha * B.q[c];
+        double sv = EXACT ? B.r[c] - alpha * B.q[c] : __fma_rn(-alpha, B.q[c], B.r[c]);
         B.s[c] = sv;
-        B.ss[c] = first_sweep ? 0.0 + (sv - 0.0) / diag(C, cc, i) : 0.0;
+        if (!first_sweep) {
+            B.ss[c] = 0.0;
+        } else {
+            double ac = diag<EXACT>(C.xpart[i], cc, C);
+            B.ss[c] = EXACT ? 0.0 + (sv - 0.0) / ac : sv * fast_rcp(ac);
+        }
     }
     SEGMENT_END
 }
 
 // x += alpha pp + omega ss; r = s - omega t (src/eq.h:385-395) with
 // <r0, r> and <r, r> for the finisher.
+template <bool EXACT>
 __global__ void __launch_bounds__(TILE_THREADS)
 k_bicg_xr(Grid g, Segments S, PoissonBufs B, const double *ppf, const double *ssf, int seq,
           Partials<2> part, KrylovState *st) {
@@ -185,8 +246,14 @@ k_bicg_xr(Grid g, Segments S, PoissonBufs B, const double *ppf, const double *ss
     SEGMENT_LOOP(S)
     long long c = c0;
     for (int i = i0; i < i1; i++, c += g.sx) {
-        B.x[c] = B.x[c] + alpha * ppf[c] + omega * ssf[c];
-        double rv = B.s[c] - omega * B.t[c];
+        double rv;
+        if (EXACT) {
+            B.x[c] = B.x[c] + alpha * ppf[c] + omega * ssf[c];
+            rv = B.s[c] - omega * B.t[c];
+        } else {
+            B.x[c] = __fma_rn(omega, ssf[c], __fma_rn(alpha, ppf[c], B.x[c]));
+            rv = __fma_rn(-omega, B.t[c], B.s[c]);
+        }
         B.r[c] = rv;
         r0r += B.r0[c] * rv;
         rr += rv * rv;
@@ -197,10 +264,10 @@ k_bicg_xr(Grid g, Segments S, PoissonBufs B, const double *ppf, const double *ss
     if (grid_reduce<2>(vals, 0u, part) && threadIdx.x == 0) fin_xr(st, vals[0], vals[1]);
 }
 
-
 // ------------------------------------------------------- TMA stencil sweeps
 
-constexpr int NSTAGE = 6;
+constexpr int NSTAGE = 8;
+constexpr int MAXCHUNK = 32;                  // Segments caps a chunk at 32 planes
 constexpr int HK = 2;                         // halo in k: 16 bytes of FP64
 constexpr int TKW = TK + 2 * HK;              // 36
 constexpr int TJW = TJ + 2;                   // 10
@@ -231,9 +298,9 @@ struct StencilArgs {
 // One block = one column segment.  Load L (0 <= L < nplanes + 2) brings
 // plane i0 - 1 + L of the operand (halo box) and, for the planes the block
 // computes, of the point-wise input (plain box) into ring stage L % NSTAGE.
-// Plane i0 + n is computed from loads n, n + 1, n + 2; after it, its stage
-// (load n) is refilled with load n + NSTAGE.
-template <int KIND>
+// Plane i0 + n is computed from loads n, n + 1, n + 2.  Each pass computes
+// two planes and then refills the two stages it released.
+template <int KIND, bool EXACT>
 __global__ void __launch_bounds__(TILE_THREADS)
 k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m_op,
           const __grid_constant__ CUtensorMap m_pw, StencilArgs A, Partials<2> part,
@@ -241,6 +308,7 @@ k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
     if (KIND != SK_INIT && st->done) return;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) unsigned long long bar[NSTAGE];
+    __shared__ double s_ae[MAXCHUNK], s_aw[MAXCHUNK], s_xp[MAXCHUNK];
     const int u = blockIdx.x;
     int i0, i1, j, k;
     const bool active = S.column(u, i0, i1, j, k);
@@ -253,6 +321,11 @@ k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
     if (threadIdx.x == 0) {
         for (int s = 0; s < NSTAGE; s++) mbar_init(&bar[s], 1);
         fence_barrier_init();
+    }
+    if (threadIdx.x < nplanes) {
+        s_ae[threadIdx.x] = C.ae[i0 + threadIdx.x];
+        s_aw[threadIdx.x] = C.aw[i0 + threadIdx.x];
+        s_xp[threadIdx.x] = C.xpart[i0 + threadIdx.x];
     }
     __syncthreads();
     auto issue = [&](int L) {
@@ -270,55 +343,66 @@ k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
     ColumnCoef cc;
     if (active) cc = column_coef(C, j, k);
     const int idx = (warp + 1) * TKW + lane + HK;
+    const int sx = (int)g.sx;
+    const int cbase = active ? (int)g.at(i0, j, k) : 0;
     double acc0 = 0, acc1 = 0;
+
+    // one cell of plane i0 + nn
+    auto cell = [&](int nn) {
+        const double *W = (const double *)(smem + (nn % NSTAGE) * STAGE_BYTES);
+        const double *Cp = (const double *)(smem + ((nn + 1) % NSTAGE) * STAGE_BYTES);
+        const double *E = (const double *)(smem + ((nn + 2) % NSTAGE) * STAGE_BYTES);
+        const double pw = ((const double *)((const unsigned char *)Cp + OP_BYTES_PAD))[warp * TK + lane];
+        const int c = cbase + nn * sx;
+        const double xc = Cp[idx];
+        const double ac = diag<EXACT>(s_xp[nn], cc, C);
+        const double ax = apply_a<EXACT>(ac, s_ae[nn], s_aw[nn], cc, xc, E[idx], W[idx],
+                                         Cp[idx + TKW], Cp[idx - TKW], Cp[idx + 1], Cp[idx - 1]);
+        if (KIND == SK_JACOBI) {
+            A.out[c] = xc + relax<EXACT>(pw, ax, ac);
+        } else if (KIND == SK_RESIDUAL) {
+            double r = pw - ax;
+            acc0 += r * r;
+            if (A.out) A.out[c] = r;
+            if (A.out2) A.out2[c] = xc;
+        } else if (KIND == SK_INIT) {
+            double r = pw - ax;
+            A.out[c] = r;
+            A.out2[c] = r;
+            A.out3[c] = 0;
+            acc0 += r * r;
+        } else if (KIND == SK_Q) {
+            A.out[c] = ax;
+            acc0 += pw * ax;
+        } else if (KIND == SK_T) {
+            A.out[c] = ax;
+            acc0 += ax * pw;
+            acc1 += ax * ax;
+        } else if (KIND == SK_SOR) {
+            const int i = i0 + nn;
+            if (((i + j + k) & 1) == A.color) {
+                double rel = relax<EXACT>(pw, ax, ac);
+                A.out[c] = EXACT ? xc + A.w * rel : __fma_rn(A.w, rel, xc);
+            }
+        }
+    };
+
     int waited = 0;
     bool fail = false;
-    for (int n = 0; n < nplanes; n++) {
-        while (!fail && waited <= n + 2) {
+    for (int n = 0; n < nplanes; n += 2) {
+        const int m = nplanes - n < 2 ? nplanes - n : 2;
+        while (!fail && waited <= n + m + 1) {
             fail = !mbar_wait(&bar[waited % NSTAGE], (unsigned)((waited / NSTAGE) & 1));
             if (!fail) waited++;
         }
         if (!fail && active) {
-            const double *W = (const double *)(smem + (n % NSTAGE) * STAGE_BYTES);
-            const double *Cp = (const double *)(smem + ((n + 1) % NSTAGE) * STAGE_BYTES);
-            const double *E = (const double *)(smem + ((n + 2) % NSTAGE) * STAGE_BYTES);
-            const double pw = ((const double *)((const unsigned char *)Cp + OP_BYTES_PAD))[warp * TK + lane];
-            const int i = i0 + n;
-            const long long c = g.at(i, j, k);
-            const double xc = Cp[idx];
-            const double ac = diag(C, cc, i);
-            // ac*xc + ae*xe + aw*xw + an*xn + as*xs + at*xt + ab*xb, left to right
-            const double ax = ac * xc + C.ae[i] * E[idx] + C.aw[i] * W[idx] + cc.an * Cp[idx + TKW] +
-                              cc.as * Cp[idx - TKW] + cc.at * Cp[idx + 1] + cc.ab * Cp[idx - 1];
-            if (KIND == SK_JACOBI) {
-                A.out[c] = xc + (pw - ax) / ac;
-            } else if (KIND == SK_RESIDUAL) {
-                double r = pw - ax;
-                acc0 += r * r;
-                if (A.out) A.out[c] = r;
-                if (A.out2) A.out2[c] = xc;
-            } else if (KIND == SK_INIT) {
-                double r = pw - ax;
-                A.out[c] = r;
-                A.out2[c] = r;
-                A.out3[c] = 0;
-                acc0 += r * r;
-            } else if (KIND == SK_Q) {
-                A.out[c] = ax;
-                acc0 += pw * ax;
-            } else if (KIND == SK_T) {
-                A.out[c] = ax;
-                acc0 += ax * pw;
-                acc1 += ax * ax;
-            } else if (KIND == SK_SOR) {
-                if (((i + j + k) & 1) == A.color) A.out[c] = xc + A.w * ((pw - ax) / ac);
-            }
+            cell(n);
+            if (m == 2) cell(n + 1);
         }
         if (__syncthreads_or(fail)) break;
-        if (threadIdx.x == 0 && issued < nload) {
-            fence_proxy_async();  // stage n was read through the generic proxy
-            issue(issued);
-            issued++;
+        if (threadIdx.x == 0) {
+            fence_proxy_async();  // the released stages were read through the generic proxy
+            for (int q = 0; q < m && issued < nload; q++) issue(issued++);
         }
     }
     if (__syncthreads_or(fail)) {
@@ -357,16 +441,24 @@ void stencil_launch(const LaunchCtx &L, int kind_tag, const Grid &g, const Poiss
                     const PoissonConfig &cfg, const double *op, const double *pw,
                     const StencilArgs &A, Partials<2> part, KrylovState *st) {
     const Segments &S = cfg.seg;
+    const CUtensorMap &mo = cfg.maps->of(op).halo, &mp = cfg.maps->of(pw).plain;
     L.pre(kind_tag);
-    k_stencil<KIND><<<S.count, TILE_THREADS, NSTAGE * STAGE_BYTES, L.s>>>(
-        g, C, S, cfg.maps->of(op).halo, cfg.maps->of(pw).plain, A, part, st);
+    if (cfg.reference_sums)
+        k_stencil<KIND, true><<<S.count, TILE_THREADS, NSTAGE * STAGE_BYTES, L.s>>>(g, C, S, mo, mp,
+                                                                                 A, part, st);
+    else
+        k_stencil<KIND, false><<<S.count, TILE_THREADS, NSTAGE * STAGE_BYTES, L.s>>>(g, C, S, mo, mp,
+                                                                                  A, part, st);
     L.post(kind_tag);
 }
 
 }  // namespace
 
 Segments poisson_segments(const Grid &g, int sm_count) {
-    return Segments::make(interior_box(g), sm_count * 8);
+    Segments s = Segments::make(interior_box(g), sm_count * 8);
+    if (s.ich > MAXCHUNK) throw std::logic_error("segment chunk exceeds MAXCHUNK");
+    if (g.total >= (1LL << 31)) throw std::invalid_argument("grid too large for 32-bit cell offsets");
+    return s;
 }
 
 size_t poisson_stencil_smem() { return (size_t)NSTAGE * STAGE_BYTES; }
@@ -453,21 +545,24 @@ void launch_bicg_iteration(const LaunchCtx &L, const Grid &g, const PoissonCoef 
     int first = (cfg.pc == PC_JACOBI && cfg.pc_sweeps >= 1) ? 1 : 0;
     int seq = cfg.reference_sums;
     L.pre(KK_BICG_P);
-    k_bicg_p<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
+    if (seq) k_bicg_p<true><<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
+    else k_bicg_p<false><<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
     L.post(KK_BICG_P);
     double *ppf = precondition(L, g, C, cfg, B.pp, B.tp, B.pk, st);
     StencilArgs Aq{B.q, nullptr, nullptr, 0, 0, !seq};
     stencil_launch<SK_Q>(L, KK_BICG_Q, g, C, cfg, ppf, B.r0, Aq, part, st);
     if (seq) seq_launch(L, g, SEQ_Q, B.r0, B.q, nullptr, nullptr, st);
     L.pre(KK_BICG_S);
-    k_bicg_s<<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
+    if (seq) k_bicg_s<true><<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
+    else k_bicg_s<false><<<S.count, TILE_THREADS, 0, L.s>>>(g, C, S, B, first, st);
     L.post(KK_BICG_S);
     double *ssf = precondition(L, g, C, cfg, B.ss, B.ts, B.s, st);
     StencilArgs At{B.t, nullptr, nullptr, 0, 0, !seq};
     stencil_launch<SK_T>(L, KK_BICG_T, g, C, cfg, ssf, B.s, At, part, st);
     if (seq) seq_launch(L, g, SEQ_T, B.t, B.s, B.t, B.t, st);
     L.pre(KK_BICG_XR);
-    k_bicg_xr<<<S.count, TILE_THREADS, 0, L.s>>>(g, S, B, ppf, ssf, seq, part, st);
+    if (seq) k_bicg_xr<true><<<S.count, TILE_THREADS, 0, L.s>>>(g, S, B, ppf, ssf, seq, part, st);
+    else k_bicg_xr<false><<<S.count, TILE_THREADS, 0, L.s>>>(g, S, B, ppf, ssf, seq, part, st);
     L.post(KK_BICG_XR);
     if (seq) seq_launch(L, g, SEQ_XR, B.r0, B.r, B.r, B.r, st);
 }

@@ -50,8 +50,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default=CASE)
-    ap.add_argument("--e2e-steps", type=int, default=2,
-                    help="steps of the end-to-end (host buffer) measurement; 0 skips it")
+    ap.add_argument("--e2e-steps", type=int, default=-1,
+                    help="steps of the end-to-end (host buffer) measurement: -1 the same "
+                         "steps as the timed region, 0 skips it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -276,10 +277,17 @@ def run_ours(args):
         ms = float(t.item())
     value = n_int * args.steps * world / (ms / 1e3) / 1e6
 
-    # ---- end to end through the public API with host (pinned) buffers
-    e2e_steps = args.e2e_steps
+    # ---- end to end through the public API with host (pinned) buffers: a
+    # second solver replays the same warm-up and the same timed steps, each
+    # step fed from and returned to pinned host memory
+    s.finalize()
+    e2e_steps = args.steps if args.e2e_steps < 0 else min(args.e2e_steps, args.steps)
     e2e_value, h2d = None, 0
     if e2e_steps > 0:
+        s = pkg.Solver(tmp, device=local)
+        s.set_inflow_profile(prof)
+        s.set_state(U0)
+        s.step(max(args.warmup, 1))
         U_h = torch.empty(s._shape(3), dtype=torch.float64).pin_memory().numpy()
         p_h = torch.empty(s._shape(1), dtype=torch.float64).pin_memory().numpy()
         s.field("U", out=U_h)
@@ -288,15 +296,19 @@ def run_ours(args):
         torch.cuda.synchronize()
         s.synchronize()
         w0 = time.perf_counter()
+        e2e_its = []
         for _ in range(e2e_steps):
             s.set_field("U", U_h)
             s.set_field("p", p_h)
             s.step(1)
             s.field("U", out=U_h)
             s.field("p", out=p_h)
-            s.stats()
+            e2e_its.append(s.stats()["it"])
         s.synchronize()
         e2e_s = time.perf_counter() - w0
+        if e2e_its != its[:e2e_steps]:
+            raise RuntimeError(f"end-to-end replay took other iteration counts {e2e_its} "
+                               f"than the timed region {its[:e2e_steps]}")
         if world > 1:
             t = torch.tensor([e2e_s], device="cuda")
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
