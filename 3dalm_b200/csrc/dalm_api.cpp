@@ -423,8 +423,9 @@ struct dalm_handle {
         // solve's count; later batches grow with the count so far.  Kernels
         // enqueued after convergence return at once.
         long long issued = 0;
-        long long batch = opt.poisson_batch > 0 ? opt.poisson_batch
-                                                : (last_it > 12 ? last_it - 8 : 4);
+        long long batch = opt.poisson_batch > 0
+                              ? opt.poisson_batch
+                              : std::min<long long>(256, last_it > 12 ? last_it / 2 : 4);
         while (true) {
             batch = std::min<long long>(batch, std::max<long long>(1, max_it - issued));
             for (long long n = 0; n < batch; n++) enqueue_poisson_iteration();
@@ -436,7 +437,7 @@ struct dalm_handle {
             if (issued > max_it + 1)
                 throw std::runtime_error("Poisson loop did not stop at its iteration limit");
             batch = opt.poisson_batch > 0 ? opt.poisson_batch
-                                          : std::max<long long>(4, std::min<long long>(64, issued / 16));
+                                          : std::max<long long>(8, std::min<long long>(96, issued / 8));
         }
         last_it = h_kst->it;
     }
