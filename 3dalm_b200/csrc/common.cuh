@@ -35,6 +35,11 @@ struct DeviceWaitError : std::runtime_error {
     explicit DeviceWaitError(const std::string &m) : std::runtime_error(m) {}
 };
 
+// An option combination this build does not implement (DALM_ERR_UNSUPPORTED).
+struct Unsupported : std::runtime_error {
+    explicit Unsupported(const std::string &m) : std::runtime_error(m) {}
+};
+
 // Sets the message returned by dalm_last_error(NULL).
 void set_last_error(const std::string &msg);
 

@@ -7,6 +7,8 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -79,6 +81,7 @@ struct dalm_handle {
     double *partial = nullptr;
     unsigned int *ticket = nullptr;
     KrylovState *d_kst = nullptr, *h_kst = nullptr;
+    bool trace = false;  // DALM_TRACE_POISSON=1: one stderr line per pressure solve
     DiagState *d_diag = nullptr, *h_diag = nullptr;
     double *d_prof = nullptr;
     // actuator line
@@ -200,10 +203,16 @@ struct dalm_handle {
     // ---- construction ----------------------------------------------------
     void init(const std::string &dir, const dalm_options &o) {
         opt = o;
-        if (opt.precision != DALM_FP64)
-            throw std::invalid_argument("only DALM_FP64 precision is available in this build");
-        if (opt.limiter != DALM_LIMITER_MINMOD)
-            throw std::invalid_argument("only the minmod limiter is available in this build");
+        if (opt.precision == DALM_MIXED)
+            throw Unsupported("DALM_MIXED is not implemented: FP32 in the pressure solve needs "
+                              "more BiCGStab iterations than it saves and breaks down on "
+                              "stretched meshes");
+        if (opt.precision != DALM_FP64) throw std::invalid_argument("unknown precision");
+        if (opt.limiter == DALM_LIMITER_VAN_ALBADA)
+            throw Unsupported("the van Albada limiter is not implemented in this build");
+        if (opt.limiter != DALM_LIMITER_MINMOD) throw std::invalid_argument("unknown limiter");
+        const char *tr = std::getenv("DALM_TRACE_POISSON");
+        trace = tr && tr[0] == '1';
         cs = load_case(dir);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -440,6 +449,9 @@ struct dalm_handle {
                                           : std::max<long long>(8, std::min<long long>(96, issued / 8));
         }
         last_it = h_kst->it;
+        if (trace)
+            std::fprintf(stderr, "[dalm] step %lld poisson it %lld err %.3e\n", (long long)step,
+                         (long long)last_it, h_kst->err);
     }
     void stage_project() {
         StageTimer t(this, DALM_STAGE_PROJECT);
@@ -663,6 +675,10 @@ struct dalm_handle {
         (h)->err = e.what();                           \
         return DALM_ERR_DEVICE_WAIT;                   \
     }                                                  \
+    catch (const Unsupported &e) {                     \
+        (h)->err = e.what();                           \
+        return DALM_ERR_UNSUPPORTED;                   \
+    }                                                  \
     catch (const std::invalid_argument &e) {           \
         (h)->err = e.what();                           \
         return DALM_ERR_ARG;                           \
@@ -704,6 +720,9 @@ int dalm_create(const char *case_dir, const dalm_options *opt, dalm_handle **out
     } catch (const CudaError &e) {
         g_last_error = e.what();
         return DALM_ERR_CUDA;
+    } catch (const Unsupported &e) {
+        g_last_error = e.what();
+        return DALM_ERR_UNSUPPORTED;
     } catch (const std::invalid_argument &e) {
         g_last_error = e.what();
         return DALM_ERR_ARG;

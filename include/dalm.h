@@ -41,14 +41,19 @@ extern "C" {
 /* ---- enums ------------------------------------------------------------ */
 enum dalm_precision {
     DALM_FP64 = 0,        /* every stage in FP64, the reference's arithmetic */
-    DALM_MIXED = 1        /* FP32 stencil bulk + FP32 inner Krylov under FP64
-                             iterative refinement; FP64 dots/norms/pressure  */
+    DALM_MIXED = 1        /* reserved: dalm_create returns
+                             DALM_ERR_UNSUPPORTED.  FP32 in the pressure
+                             solve (inner solves under FP64 refinement, or
+                             an FP32 preconditioner) was measured to need
+                             more BiCGStab iterations than it saves, and to
+                             break down, on stretched meshes.           */
 };
 
 enum dalm_limiter {
     DALM_LIMITER_MINMOD = 0,    /* the reference's b=4 minmod-type limiter,
                                    src/cfd.h:37-54                           */
-    DALM_LIMITER_VAN_ALBADA = 1 /* smooth limiter (extension)               */
+    DALM_LIMITER_VAN_ALBADA = 1 /* reserved for a smooth limiter (not in the
+                                   reference): DALM_ERR_UNSUPPORTED       */
 };
 
 /* Fields addressable by dalm_get_field / dalm_set_field (reference arrays). */

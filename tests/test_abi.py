@@ -91,3 +91,16 @@ def test_solver_without_gpu_fails_loudly(make_case):
     spec, mesh, d, U0, prof = make_case("tiny-sor")
     with pytest.raises(pkg.DalmError):
         pkg.Solver(d)
+
+
+def test_reserved_options_report_unsupported(lib, make_case):
+    pkg = package()
+    spec, mesh, d, U0, prof = make_case("tiny-bicg")
+    for field, value, word in (("precision", pkg.MIXED, b"DALM_MIXED"),
+                               ("limiter", pkg.VAN_ALBADA, b"van Albada")):
+        o = pkg.Options()
+        lib.dalm_default_options(C.byref(o))
+        setattr(o, field, value)
+        h = C.c_void_p()
+        assert lib.dalm_create(d.encode(), C.byref(o), C.byref(h)) == 6 and not h.value
+        assert word in lib.dalm_last_error(None)
