@@ -53,7 +53,8 @@ class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("limiter", C.c_int), ("device", C.c_int),
                 ("time_average", C.c_int), ("check_finite", C.c_int),
                 ("poisson_batch", C.c_int), ("use_graphs", C.c_int), ("profile", C.c_int),
-                ("reference_sums", C.c_int), ("reserved", C.c_int * 7)]
+                ("reference_sums", C.c_int), ("fused_krylov", C.c_int),
+                ("refine_inner_it", C.c_int), ("reserved", C.c_int * 5)]
 
 
 _PD = C.POINTER(C.c_double)
@@ -94,7 +95,8 @@ class Solver:
 
     def __init__(self, case_dir: str | None = None, precision: int = FP64, device: int = 0,
                  time_average: bool = True, profile: bool = False, poisson_batch: int = 0,
-                 limiter: int = MINMOD, reference_sums: bool = False):
+                 limiter: int = MINMOD, reference_sums: bool = False, fused_krylov: bool = True,
+                 refine_inner_it: int = 0):
         self.lib = load_library()
         self.h = C.c_void_p()
         self.opt = Options()
@@ -106,6 +108,8 @@ class Solver:
         self.opt.profile = int(profile)
         self.opt.poisson_batch = poisson_batch
         self.opt.reference_sums = int(reference_sums)
+        self.opt.fused_krylov = int(fused_krylov)
+        self.opt.refine_inner_it = int(refine_inner_it)
         if case_dir is not None:
             self.initialize(case_dir)
 

@@ -244,7 +244,10 @@ enum KernelKind {
     KK_ALM_POINTS, KK_ALM_SUMS, KK_ALM_PROJECT,
     KK_SOR_SWEEP, KK_RESIDUAL_NORM, KK_JACOBI_SWEEP,
     KK_BICG_INIT, KK_BICG_P, KK_BICG_Q, KK_BICG_S, KK_BICG_T, KK_BICG_XR,
-    KK_POISSON_BEGIN, KK_LAYOUT, KK_SEQ_SUM, KK_COUNT
+    KK_POISSON_BEGIN, KK_LAYOUT, KK_SEQ_SUM, KK_BICG_PF, KK_BICG_SF, KK_REFINE_RESIDUAL, KK_REFINE_UPDATE,
+    // FP32 inner solves of iterative refinement
+    KK_SOR_SWEEP32, KK_JACOBI_SWEEP32, KK_BICG_P32, KK_BICG_Q32, KK_BICG_S32, KK_BICG_T32, KK_BICG_XR32,
+    KK_COUNT
 };
 
 // Everything a launcher needs besides its operands: the stream, the number

@@ -29,13 +29,23 @@ constexpr double PI_D = 3.14159265358979323846;
 // Truncation radius of the Gaussian projection: r^2 <= 40 eps^2, where the
 // dropped weight exp(-40) ~ 4e-18 of the peak is below FP64 resolution of f.
 constexpr double ALM_CUTOFF_EPS2 = 40.0;
+// Iterative refinement (DALM_MIXED): an FP32 inner solve stops at
+// INNER_RTOL x the FP64 residual or after the pass cap (refine_inner_it,
+// default INNER_CAP iterations); a pass that shrinks the FP64 residual by
+// less than 1/STALL hands the rest of the solve to the FP64 solver.
+constexpr double INNER_RTOL = 1e-3;
+constexpr long long INNER_CAP = 50;
+constexpr double STALL = 0.85;
+constexpr long long MAX_REFINE = 1000;
 
 const char *kKindNames[KK_COUNT] = {
     "predict", "flux_rhs", "pressure_bc", "project", "velocity_bc", "diag", "tavg",
     "alm_points", "alm_sums", "alm_project",
     "sor_sweep", "residual_norm", "jacobi_sweep",
     "bicg_init", "bicg_p", "bicg_q", "bicg_s", "bicg_t", "bicg_xr",
-    "poisson_begin", "layout", "seq_sum"};
+    "poisson_begin", "layout", "seq_sum", "bicg_p_fused", "bicg_s_fused", "refine_residual",
+    "refine_update", "sor_sweep32", "jacobi_sweep32", "bicg_p32", "bicg_q32", "bicg_s32",
+    "bicg_t32", "bicg_xr32"};
 
 }  // namespace
 
@@ -76,6 +86,12 @@ struct dalm_handle {
     double *scratch = nullptr;   // one scalar field for nut / div output
     double *staging = nullptr;   // reference-layout staging buffer (3*len)
     PoissonBufs pb{};
+    PoissonBufsT<float> pbf{};  // inner solves A e = r of iterative refinement (DALM_MIXED)
+    bool mixed = false;
+    long long refine_fp32_it = 0, refine_fp64_it = 0, refine_passes = 0;  // last solve
+    std::vector<long long> last_inner;  // inner iterations per refinement pass, last solve
+    FusedBufs fb{};
+    bool fused = false;  // BiCGStab iterations as fused half-iteration kernels
     PoissonConfig pcfg{};
     MapTable maps;
     double *partial = nullptr;
@@ -203,11 +219,8 @@ struct dalm_handle {
     // ---- construction ----------------------------------------------------
     void init(const std::string &dir, const dalm_options &o) {
         opt = o;
-        if (opt.precision == DALM_MIXED)
-            throw Unsupported("DALM_MIXED is not implemented: FP32 in the pressure solve needs "
-                              "more BiCGStab iterations than it saves and breaks down on "
-                              "stretched meshes");
-        if (opt.precision != DALM_FP64) throw std::invalid_argument("unknown precision");
+        if (opt.precision != DALM_FP64 && opt.precision != DALM_MIXED)
+            throw std::invalid_argument("unknown precision");
         if (opt.limiter == DALM_LIMITER_VAN_ALBADA)
             throw Unsupported("the van Albada limiter is not implemented in this build");
         if (opt.limiter != DALM_LIMITER_MINMOD) throw std::invalid_argument("unknown limiter");
@@ -260,17 +273,41 @@ struct dalm_handle {
         pcfg.pc_sweeps = (int)cs.pc_max_it;
         pcfg.reference_sums = opt.reference_sums ? 1 : 0;
         pcfg.seg = poisson_segments(g, sm_count);
+        fused = opt.fused_krylov && fused_bicg_available(pcfg);
+        // FP32 inner solves exist for BiCGStab only; SOR and Jacobi solves
+        // stay FP64 under DALM_MIXED
+        mixed = opt.precision == DALM_MIXED && pcfg.method == PM_BICG;
+        if (mixed) {
+            float **kv32[] = {&pbf.x, &pbf.r, &pbf.r0, &pbf.pk, &pbf.q, &pbf.s, &pbf.t,
+                              &pbf.pp, &pbf.ss, &pbf.tp, &pbf.ts};
+            for (auto v : kv32) *v = dalloc<float>(n);
+            pbf.b = pbf.r0;  // e starts at 0, so the inner r0 = r = b
+        }
+        fb = FusedBufs{{pb.pk, nullptr}, {pb.q, nullptr}};
+        if (fused) {
+            fb.pk[1] = dalloc<double>(n);
+            fb.q[1] = dalloc<double>(n);
+        }
         const double *tma_fields[] = {pb.x, pb.b, pb.r, pb.r0, pb.pk, pb.q,
                                       pb.s, pb.t, pb.pp, pb.ss, pb.tp, pb.ts};
         for (const double *v : tma_fields) maps.add(g, v);
+        if (fused) {
+            maps.add(g, fb.pk[1]);
+            maps.add(g, fb.q[1]);
+        }
+        if (mixed) {
+            const float *tma32[] = {pbf.x, pbf.r, pbf.r0, pbf.pk, pbf.q, pbf.s,
+                                    pbf.t, pbf.pp, pbf.ss, pbf.tp, pbf.ts};
+            for (const float *v : tma32) maps.add(g, v, 4);
+        }
         pcfg.maps = &maps;
         partial = dalloc<double>((size_t)std::max(L.blocks, pcfg.seg.count) * 4);
         ticket = dalloc<unsigned int>(1);
-        d_kst = dalloc<KrylovState>(1);
+        d_kst = dalloc<KrylovState>(2);  // [0] the solve (refinement: outer), [1] inner
         d_diag = dalloc<DiagState>(1);
-        DALM_CUDA(cudaHostAlloc((void **)&h_kst, sizeof(KrylovState), cudaHostAllocDefault));
+        DALM_CUDA(cudaHostAlloc((void **)&h_kst, 2 * sizeof(KrylovState), cudaHostAllocDefault));
         DALM_CUDA(cudaHostAlloc((void **)&h_diag, sizeof(DiagState), cudaHostAllocDefault));
-        memset(h_kst, 0, sizeof(KrylovState));
+        memset(h_kst, 0, 2 * sizeof(KrylovState));
         memset(h_diag, 0, sizeof(DiagState));
         DiagState d0{};
         d0.ncell = (double)g.ni() * g.nj() * g.nk();
@@ -412,46 +449,132 @@ struct dalm_handle {
         StageTimer t(this, DALM_STAGE_FLUX_RHS);
         launch_flux_rhs(L, P, c(u_cur()), ju_cur(), B);
     }
-    void enqueue_poisson_iteration() {
-        if (pcfg.method == PM_BICG) {
-            launch_bicg_iteration(L, g, coef, pb, pcfg, Partials<2>{partial, ticket}, d_kst);
+    // iteration n (from 0) of the current solve
+    void enqueue_poisson_iteration(long long n) {
+        if (fused) {
+            launch_bicg_iteration_fused(L, g, coef, pb, fb, n, pcfg, Partials<2>{partial, ticket}, d_kst);
+        } else if (pcfg.method == PM_BICG) {
+            launch_bicg_iteration<double>(L, g, coef, pb, pcfg, Partials<2>{partial, ticket}, d_kst);
         } else if (pcfg.method == PM_SOR) {
             launch_sor_iteration(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
         } else {
             launch_jacobi_iteration(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
         }
     }
-    void stage_poisson() {
-        StageTimer t(this, DALM_STAGE_POISSON);
-        double ncell = (double)g.ni() * g.nj() * g.nk();
-        launch_poisson_begin(L, d_kst, max_it, tol, ncell);
-        if (pcfg.method == PM_BICG)
-            launch_bicg_init(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
-        // Enqueue iterations in batches and poll the device's `done` flag in
-        // between.  The first batch stops a little short of the previous
-        // solve's count; later batches grow with the count so far.  Kernels
-        // enqueued after convergence return at once.
+    void fetch_states() {
+        DALM_CUDA(cudaMemcpyAsync(h_kst, d_kst, 2 * sizeof(KrylovState), cudaMemcpyDeviceToHost, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        if (h_kst[0].wait_error || h_kst[1].wait_error)
+            throw DeviceWaitError("a TMA stage wait in the Poisson solver ran out");
+    }
+    // Enqueues iterations of solve `which` in batches and polls the device's
+    // `done` flag in between.  The first batch stops a little short of
+    // `hint` (the previous comparable solve's count); later batches grow
+    // with the count so far.  Kernels enqueued after convergence return at
+    // once.  Returns the iterations the solve took.
+    long long run_batches(int which, long long hint, long long cap) {
+        KrylovState *st = d_kst + which;
         long long issued = 0;
         long long batch = opt.poisson_batch > 0
                               ? opt.poisson_batch
-                              : std::min<long long>(256, last_it > 12 ? last_it / 2 : 4);
+                              : std::min<long long>(256, hint > 12 ? hint / 2 : 4);
         while (true) {
-            batch = std::min<long long>(batch, std::max<long long>(1, max_it - issued));
-            for (long long n = 0; n < batch; n++) enqueue_poisson_iteration();
+            batch = std::min<long long>(batch, std::max<long long>(1, cap - issued));
+            for (long long n = 0; n < batch; n++) {
+                if (which == 1)
+                    launch_bicg_iteration<float>(L, g, coef, pbf, pcfg, Partials<2>{partial, ticket}, st);
+                else
+                    enqueue_poisson_iteration(issued + n);
+            }
             issued += batch;
-            DALM_CUDA(cudaMemcpyAsync(h_kst, d_kst, sizeof(KrylovState), cudaMemcpyDeviceToHost, stream));
-            DALM_CUDA(cudaStreamSynchronize(stream));
-            if (h_kst->wait_error) throw DeviceWaitError("a TMA stage wait in the Poisson solver ran out");
-            if (h_kst->done) break;
-            if (issued > max_it + 1)
+            fetch_states();
+            if (h_kst[which].done) break;
+            if (issued > cap + 1)
                 throw std::runtime_error("Poisson loop did not stop at its iteration limit");
             batch = opt.poisson_batch > 0 ? opt.poisson_batch
                                           : std::max<long long>(8, std::min<long long>(96, issued / 8));
         }
-        last_it = h_kst->it;
+        return h_kst[which].it;
+    }
+    // The reference's solve (FP64) from the current p; `used` iterations of
+    // the case's cap are already spent.
+    void solve_fp64(long long used) {
+        double ncell = (double)g.ni() * g.nj() * g.nk();
+        launch_poisson_begin(L, d_kst, max_it - used, tol, ncell);
+        if (pcfg.method == PM_BICG)
+            launch_bicg_init(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
+        long long hint = mixed ? refine_fp64_it : last_it;
+        long long n = run_batches(0, hint, max_it - used);
+        refine_fp64_it = n;
+        h_kst[0].it = used + n;
+    }
+    void stage_poisson() {
+        StageTimer t(this, DALM_STAGE_POISSON);
+        if (!mixed) {
+            solve_fp64(0);
+        } else {
+            solve_mixed();
+        }
+        last_it = h_kst[0].it;
         if (trace)
-            std::fprintf(stderr, "[dalm] step %lld poisson it %lld err %.3e\n", (long long)step,
-                         (long long)last_it, h_kst->err);
+            std::fprintf(stderr, "[dalm] step %lld poisson it %lld err %.3e (FP32 %lld in %lld passes, FP64 %lld)\n",
+                         (long long)step, (long long)last_it, h_kst[0].err, refine_fp32_it,
+                         refine_passes, mixed ? refine_fp64_it : last_it);
+    }
+    // Iterative refinement (DALM_MIXED): r = b - A p and its norm in FP64;
+    // an FP32 BiCGStab solve of A e = r from e = 0, capped at the pass cap;
+    // p += e; repeat until the FP64 residual meets the tolerance.  A pass
+    // that makes the residual worse is taken back; a pass that breaks down,
+    // or gains less than 1/STALL, ends the refinement and the reference's
+    // FP64 solve finishes from the current p.
+    void solve_mixed() {
+        const double ncell = (double)g.ni() * g.nj() * g.nk();
+        const long long cap = opt.refine_inner_it > 0 ? opt.refine_inner_it : INNER_CAP;
+        launch_poisson_begin(L, d_kst, max_it, tol, ncell, MAX_REFINE, INNER_RTOL, cap);
+        launch_poisson_begin(L, d_kst + 1, max_it, tol, ncell, 0, 0, 0, 1);
+        launch_refine_residual(L, g, coef, pcfg, Pp, B, pbf, Partials<2>{partial, ticket}, d_kst,
+                               d_kst + 1);
+        fetch_states();
+        double prev = h_kst[0].err;
+        refine_fp32_it = 0;
+        refine_fp64_it = 0;
+        refine_passes = 0;
+        bool fallback = false;
+        long long used = 0;
+        size_t pass = 0;
+        while (!h_kst[0].done) {
+            if (last_inner.size() <= pass) last_inner.push_back(0);
+            last_inner[pass] = run_batches(1, last_inner[pass], cap);
+            refine_fp32_it += h_kst[1].it;
+            refine_passes = (long long)pass + 1;
+            if (h_kst[1].breakdown) {  // the correction is discarded, p unchanged
+                used = h_kst[0].it + h_kst[1].it;
+                fallback = true;
+                break;
+            }
+            launch_refine_update(L, g, pcfg, Pp, pbf.x, 1.0);
+            launch_refine_residual(L, g, coef, pcfg, Pp, B, pbf, Partials<2>{partial, ticket},
+                                   d_kst, d_kst + 1);
+            fetch_states();
+            const double now = h_kst[0].err;
+            if (trace)
+                std::fprintf(stderr, "[dalm]   pass %zu FP32 it %lld -> residual %.3e\n", pass,
+                             last_inner[pass], now);
+            if (!(now < prev)) {  // worse (or not finite): take the correction back
+                launch_refine_update(L, g, pcfg, Pp, pbf.x, -1.0);
+                used = h_kst[0].it;
+                fallback = true;
+                break;
+            }
+            if (!h_kst[0].done && now > STALL * prev) {
+                used = h_kst[0].it;
+                fallback = true;
+                break;
+            }
+            prev = now;
+            pass++;
+        }
+        if (fallback && used < max_it) solve_fp64(used);
     }
     void stage_project() {
         StageTimer t(this, DALM_STAGE_PROJECT);
@@ -703,6 +826,8 @@ void dalm_default_options(dalm_options *opt) {
     opt->use_graphs = 1;
     opt->profile = 0;
     opt->reference_sums = 0;
+    opt->fused_krylov = 1;
+    opt->refine_inner_it = 0;
 }
 
 int dalm_create(const char *case_dir, const dalm_options *opt, dalm_handle **out) {
@@ -979,6 +1104,18 @@ int dalm_get_kernel_timing(dalm_handle *h, int index, const char **name, int64_t
         case KK_BICG_S: s = 4 * n; break;
         case KK_BICG_T: s = 3 * n; break;
         case KK_BICG_XR: s = 8 * n; break;
+        case KK_BICG_PF: s = 7 * n; break;
+        case KK_BICG_SF: s = 5 * n; break;
+        case KK_REFINE_RESIDUAL: s = 3.5 * n; break;  // R x, b (FP64); W r, r0, q (FP32)
+        case KK_REFINE_UPDATE: s = 2.5 * n; break;    // R x, e; W x
+        // FP32 vectors: half the scalars' bytes
+        case KK_SOR_SWEEP32: s = 2 * n / 2.0; break;
+        case KK_JACOBI_SWEEP32: s = 3 * n / 2.0; break;
+        case KK_BICG_P32: s = 5 * n / 2.0; break;
+        case KK_BICG_Q32: s = 3 * n / 2.0; break;
+        case KK_BICG_S32: s = 4 * n / 2.0; break;
+        case KK_BICG_T32: s = 3 * n / 2.0; break;
+        case KK_BICG_XR32: s = 8 * n / 2.0; break;
         default: s = 0; break;
         }
         *bytes_per_launch = 8.0 * s;

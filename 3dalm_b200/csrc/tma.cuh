@@ -1,12 +1,13 @@
 // TMA (cp.async.bulk.tensor) plane staging for the stencil kernels.
 //
 // A field is described to the TMA unit as a 3-D tensor {x = k + off (the
-// padded row), y = j, z = i}.  Two maps per field: `halo` boxes of
+// padded row), y = j, z = i}.  Three maps per field: `halo` boxes of
 // (32 + 2h) x 10 x 1 elements (the 32 x 8 tile of a block plus one cell in
 // j and h cells in k each side, h = 16 B / element size so that the box
-// starts on a 16-byte boundary), and `plain` boxes of 32 x 8 x 1.  Loads
-// complete on an mbarrier per ring stage.  Every wait is bounded: after
-// WAIT_LIMIT polls the kernel raises an error flag and returns.
+// starts on a 16-byte boundary), `plain` boxes of 32 x 8 x 1 and `wide`
+// boxes (below).  Loads complete on an mbarrier per ring stage.  Every wait
+// is bounded: after WAIT_LIMIT polls the kernel raises an error flag and
+// returns.
 #pragma once
 
 #include <cuda.h>
@@ -15,9 +16,15 @@
 
 namespace dalm {
 
+// `wide` boxes carry the three-cell halo of the fused BiCGStab kernels:
+// (32 + 2*4) x (8 + 2*3) x 1, starting 4 cells below the tile in k (a
+// 16-byte boundary for 4- and 8-byte elements) and 3 rows below it in j.
+constexpr int WIDE_HK = 4, WIDE_HJ = 3;
+
 struct FieldMaps {
     CUtensorMap halo;
     CUtensorMap plain;
+    CUtensorMap wide;
 };
 
 // Builds both maps for one field (element size 4 or 8) over grid g; throws

@@ -49,6 +49,7 @@ FieldMaps make_field_maps(const Grid &g, const void *base, int elem_bytes) {
     int h = 16 / elem_bytes;
     encode(&m.halo, g, base, elem_bytes, (cuuint32_t)(TK + 2 * h), (cuuint32_t)(TJ + 2));
     encode(&m.plain, g, base, elem_bytes, (cuuint32_t)TK, (cuuint32_t)TJ);
+    encode(&m.wide, g, base, elem_bytes, (cuuint32_t)(TK + 2 * WIDE_HK), (cuuint32_t)(TJ + 2 * WIDE_HJ));
     return m;
 }
 

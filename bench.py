@@ -20,6 +20,7 @@ its own GPU (the path has no exchange step on one domain): weak scaling, no
 collective on the data path; the time is the max over ranks.
 """
 import argparse
+import contextlib
 import importlib
 import json
 import os
@@ -35,12 +36,48 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s"
 CASE = "c4"
+SAMPLE_N = (256, 128, 64)  # interior cells of the CPU baseline's sample
 
-# Poisson iteration counts of the first integrating steps of this workload
-# (seed 0), measured by this benchmark's GPU arm; the FP64 GPU path and the
-# reference take the same number of iterations (tests/test_gpu_parity.py),
-# so the reference arm's per-step time model uses them.
-C4_ITERATIONS = None  # filled from a measured run; None -> use the sample's own count
+# BiCGStab iterations of each time step of this workload (seed 0, step 0
+# has no pressure solve), measured by this benchmark's GPU arm in its default
+# fast mode.  The reference's counts on the same steps differ only by the
+# summation-order spread (tests/test_oracle_sensitivity.py), so the reference
+# arm times its CPU code per iteration and per cell and models the steps the
+# GPU arm times (steps W .. W+K-1) with these counts.
+C4_ITERATIONS = [0, 1337, 1141, 274, 308, 1747, 2685]
+
+
+def step_iterations(warmup, steps):
+    """Mean iteration count of the timed steps warmup .. warmup+steps-1, or
+    None when they lie beyond the measured list."""
+    sel = C4_ITERATIONS[warmup:warmup + steps]
+    return statistics.mean(sel) if len(sel) == steps and steps > 0 else None
+
+
+def workload_config(case, cells, iterations, world):
+    """The `config` object both arms report."""
+    return {"workload": "3-turbine 512x256x128 LES step (Jacobi(3)-BiCGStab to 1e-8, log-law "
+                        "inflow, 288 blade points)",
+            "case": case, "precision": "FP64", "cells": cells,
+            "poisson_iterations": iterations, "parallelism": f"replicas x{world}",
+            "l2": "every field > 126 MB L2 (134 MB per scalar field); no flush"}
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """Sends what native code prints to stdout (the reference's setup
+    report) to stderr, so stdout carries only the JSON line."""
+    import ctypes
+    sys.stdout.flush()
+    libc = ctypes.CDLL(None)
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
 
 
 def parse():
@@ -151,8 +188,9 @@ def make_case(name, tmp):
 def cpu_sample(kind_pref="reference", iterations=None, poisson_cap=40):
     """Time the CPU oracle (the reference compiled from its own sources when
     available, else the C restatement) stage by stage on a bounded sample:
-    the same 3-turbine case at 128x64x32 cells (262,144), one integrating
-    step with the Poisson solve capped at `poisson_cap` iterations.  The
+    the same 3-turbine case at 256x128x64 cells (2,097,152; 17 MB per field,
+    beyond one core's caches), one integrating step with the Poisson solve
+    capped at `poisson_cap` iterations.  The
     per-cell stage costs, the per-cell-per-iteration Poisson cost and the
     per-cell-per-blade-point projection cost are combined into the time of
     one full 512x256x128 step with `iterations` Poisson iterations (serial,
@@ -165,8 +203,8 @@ def cpu_sample(kind_pref="reference", iterations=None, poisson_cap=40):
         O.build()
     cg = importlib.import_module("3dalm_b200.casegen")
     full = cg.config(CASE)
-    spec = cg.config(CASE, n=(128, 64, 32), steps=10)
-    with tempfile.TemporaryDirectory() as d:
+    spec = cg.config(CASE, n=SAMPLE_N, steps=10)
+    with tempfile.TemporaryDirectory() as d, quiet_stdout():
         mesh = cg.write_case(spec, d)
         o = O.Reference(d) if kind == "reference" else O.CRestatement(d)
         prof = cg.inflow_profile(spec, mesh)
@@ -190,7 +228,8 @@ def cpu_sample(kind_pref="reference", iterations=None, poisson_cap=40):
     its = iterations if iterations else it
     step_time = n_f * (per_cell + its * per_iter) + n_f * n_pts * per_cell_point
     desc = (f"{'reference (oracle/_ref)' if kind == 'reference' else 'C restatement'} serial, "
-            f"stage-timed on the same case at 128x64x32 ({n_s} cells, {n_pts} blade points, "
+            f"stage-timed on the same case at {'x'.join(map(str, SAMPLE_N))} ({n_s} cells, "
+            f"{n_pts} blade points, "
             f"Poisson capped at {it} iterations); per-cell, per-cell-iteration and "
             f"per-cell-point costs scaled to 512x256x128 with {its:.1f} Poisson iterations/step")
     return n_f / step_time / 1e6, kind, desc, sum(t)
@@ -200,12 +239,11 @@ def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
         return
-    iters = None
-    if C4_ITERATIONS:
-        iters = statistics.mean(C4_ITERATIONS[:max(1, args.steps)])
+    iters = step_iterations(args.warmup, args.steps) if args.case == CASE else None
     vals = []
     for n in range(args.warmup + args.steps):
-        v, kind, desc, secs = cpu_sample("reference", iters)
+        # warm-up samples only page the code and data in: a short solve
+        v, kind, desc, secs = cpu_sample("reference", iters, 40 if n >= args.warmup else 4)
         if n >= args.warmup:
             vals.append(v)
     value = statistics.mean(vals)
@@ -214,10 +252,11 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 16777216 / (value * 1e6) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "3-turbine 512x256x128 LES step (Jacobi-BiCGStab 1e-8, log-law "
-                               "inflow, 288 blade points)", "case": CASE},
+        "config": workload_config(args.case, 16777216,
+                                  C4_ITERATIONS[args.warmup:args.warmup + args.steps], args.gpus),
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
-                         "sample": desc},
+                         "sample": desc + "; the reference's CPU path is serial (OpenACC/MPI "
+                                          "code built without either)"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -346,11 +385,7 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded log-law + 8% Gaussian initial field, generated case files)",
-        "config": {"workload": "3-turbine 512x256x128 LES step (Jacobi(3)-BiCGStab to 1e-8, "
-                               "log-law inflow, 288 blade points)",
-                   "case": args.case, "precision": "FP64", "cells": n_int,
-                   "poisson_iterations": its, "parallelism": f"replicas x{world}",
-                   "l2": "every field > 126 MB L2 (141 MB per scalar field); no flush"},
+        "config": workload_config(args.case, n_int, its, world),
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": h2d, "steps": e2e_steps,
                 "how": "per step: dalm_set_field(U,p) from pinned host, dalm_step(1), "

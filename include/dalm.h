@@ -41,12 +41,13 @@ extern "C" {
 /* ---- enums ------------------------------------------------------------ */
 enum dalm_precision {
     DALM_FP64 = 0,        /* every stage in FP64, the reference's arithmetic */
-    DALM_MIXED = 1        /* reserved: dalm_create returns
-                             DALM_ERR_UNSUPPORTED.  FP32 in the pressure
-                             solve (inner solves under FP64 refinement, or
-                             an FP32 preconditioner) was measured to need
-                             more BiCGStab iterations than it saves, and to
-                             break down, on stretched meshes.           */
+    DALM_MIXED = 1        /* BiCGStab pressure solve by FP64 iterative
+                             refinement with FP32 inner BiCGStab passes:
+                             residual, norms, dots and the pressure in
+                             FP64, the stop test on the FP64 residual; a
+                             pass that stalls or breaks down hands the
+                             rest of the solve to the FP64 solver.  Every
+                             other stage, and SOR / Jacobi solves, FP64. */
 };
 
 enum dalm_limiter {
@@ -103,7 +104,15 @@ typedef struct {
                              cell order instead of a parallel tree; with it
                              the FP64 step reproduces the reference's
                              rounding (slow: for parity checks)          */
-    int reserved[7];
+    int fused_krylov;     /* 1 (default): each half of a Jacobi(3)-
+                             BiCGStab iteration (update, preconditioner,
+                             SpMV, dot products) as one kernel; 0: one
+                             kernel per reference loop.  Ignored with
+                             reference_sums and other preconditioners.  */
+    int refine_inner_it;  /* DALM_MIXED: FP32 iterations per refinement
+                             pass before the FP64 residual is recomputed
+                             (0: automatic, 50)                          */
+    int reserved[5];
 } dalm_options;
 
 /* Fills *opt with the defaults (FP64, minmod, device 0, time average on,
