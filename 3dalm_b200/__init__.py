@@ -95,7 +95,7 @@ class Solver:
 
     def __init__(self, case_dir: str | None = None, precision: int = FP64, device: int = 0,
                  time_average: bool = True, profile: bool = False, poisson_batch: int = 0,
-                 limiter: int = MINMOD, reference_sums: bool = False, fused_krylov: bool = True,
+                 limiter: int = MINMOD, reference_sums: bool = False, fused_krylov: bool = False,
                  refine_inner_it: int = 0):
         self.lib = load_library()
         self.h = C.c_void_p()

@@ -34,7 +34,7 @@ constexpr double ALM_CUTOFF_EPS2 = 40.0;
 // default INNER_CAP iterations); a pass that shrinks the FP64 residual by
 // less than 1/STALL hands the rest of the solve to the FP64 solver.
 constexpr double INNER_RTOL = 1e-3;
-constexpr long long INNER_CAP = 50;
+constexpr long long INNER_CAP = 100;
 constexpr double STALL = 0.85;
 constexpr long long MAX_REFINE = 1000;
 
@@ -97,7 +97,8 @@ struct dalm_handle {
     double *partial = nullptr;
     unsigned int *ticket = nullptr;
     KrylovState *d_kst = nullptr, *h_kst = nullptr;
-    bool trace = false;  // DALM_TRACE_POISSON=1: one stderr line per pressure solve
+    bool trace = false;          // DALM_TRACE_POISSON=1: one stderr line per pressure solve
+    bool trace_batches = false;  // DALM_TRACE_POISSON=2: also one per batch of iterations
     DiagState *d_diag = nullptr, *h_diag = nullptr;
     double *d_prof = nullptr;
     // actuator line
@@ -225,7 +226,8 @@ struct dalm_handle {
             throw Unsupported("the van Albada limiter is not implemented in this build");
         if (opt.limiter != DALM_LIMITER_MINMOD) throw std::invalid_argument("unknown limiter");
         const char *tr = std::getenv("DALM_TRACE_POISSON");
-        trace = tr && tr[0] == '1';
+        trace = tr && (tr[0] == '1' || tr[0] == '2');
+        trace_batches = tr && tr[0] == '2';
         cs = load_case(dir);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -488,6 +490,9 @@ struct dalm_handle {
             }
             issued += batch;
             fetch_states();
+            if (trace_batches)
+                std::fprintf(stderr, "[dalm]     solve %d: %lld iterations, residual %.3e\n", which,
+                             (long long)h_kst[which].it, h_kst[which].err);
             if (h_kst[which].done) break;
             if (issued > cap + 1)
                 throw std::runtime_error("Poisson loop did not stop at its iteration limit");
@@ -826,7 +831,7 @@ void dalm_default_options(dalm_options *opt) {
     opt->use_graphs = 1;
     opt->profile = 0;
     opt->reference_sums = 0;
-    opt->fused_krylov = 1;
+    opt->fused_krylov = 0;
     opt->refine_inner_it = 0;
 }
 

@@ -15,6 +15,11 @@ Mcell-steps/s = interior cells x steps / time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The headline `value` is the reference's precision (FP64).  The line also
+carries `mixed`: the same timed steps with DALM_MIXED (FP64 iterative
+refinement with capped FP32 BiCGStab passes), its ratio to FP64 and both
+forms' largest final FP64 residual.
+
 With N > 1 (torchrun) every rank runs an independent replica of the case on
 its own GPU (the path has no exchange step on one domain): weak scaling, no
 collective on the data path; the time is the max over ranks.
@@ -91,6 +96,7 @@ def parse():
                     help="steps of the end-to-end (host buffer) measurement: -1 the same "
                          "steps as the timed region, 0 skips it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision timing")
     return ap.parse_args()
 
 
@@ -284,46 +290,65 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def fresh_solver(profile):
+    def fresh_solver(profile, precision=pkg.FP64):
         """A solver at the start of the timed steps: state set, warm-up run."""
-        sv = pkg.Solver(tmp, device=local, profile=profile)
+        sv = pkg.Solver(tmp, device=local, profile=profile, precision=precision)
         sv.set_inflow_profile(prof)
         sv.set_state(U0)
         sv.step(max(args.warmup, 1))
         return sv
 
-    # ---- device-resident timed region (no per-kernel instrumentation)
-    s = fresh_solver(False)
-    stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
-    s.timings(reset=True)
-    clocks = ClockSampler(local)
-    barrier()
-    torch.cuda.synchronize()
-    s.synchronize()
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    its = []
-    for _ in range(args.steps):
-        s.step(1)
-        its.append(s.stats()["it"])
-    e1.record(stream)
-    e1.synchronize()
-    s.synchronize()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    _, launches = s.timings()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    def timed_region(precision):
+        """The K timed steps on the device (CUDA events on the solver's
+        stream, no per-kernel instrumentation), max over ranks."""
+        s = fresh_solver(False, precision)
+        stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
+        s.timings(reset=True)
+        clocks = ClockSampler(local)
+        barrier()
+        torch.cuda.synchronize()
+        s.synchronize()
+        clocks.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        its, errs = [], []
+        for _ in range(args.steps):
+            s.step(1)
+            st = s.stats()
+            its.append(st["it"])
+            errs.append(st["err"])
+        e1.record(stream)
+        e1.synchronize()
+        s.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        _, launches = s.timings()
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        s.finalize()
+        return ms, its, errs, clk, launches
+
+    # ---- the reference's precision: the headline
+    ms, its, errs, clk, launches = timed_region(pkg.FP64)
     value = n_int * args.steps * world / (ms / 1e3) / 1e6
+    # ---- the mixed-precision form on the same steps
+    mixed = None
+    if not args.no_mixed:
+        mms, mits, merrs, mclk, _ = timed_region(pkg.MIXED)
+        mvalue = n_int * args.steps * world / (mms / 1e3) / 1e6
+        mixed = {"value": mvalue, "unit": METRIC, "ms_per_step": mms / args.steps,
+                 "vs_fp64": mvalue / value, "poisson_iterations": mits,
+                 "max_residual": max(merrs), "fp64_max_residual": max(errs),
+                 "tolerance": spec.tol, "clocks": mclk,
+                 "how": "DALM_MIXED: FP64 iterative refinement with capped FP32 BiCGStab passes, "
+                        "FP64 fallback when a pass stalls; stop test on the FP64 residual"}
 
     # ---- end to end through the public API with host (pinned) buffers: a
     # second solver replays the same warm-up and the same timed steps, each
     # step fed from and returned to pinned host memory
-    s.finalize()
     e2e_steps = args.steps if args.e2e_steps < 0 else min(args.e2e_steps, args.steps)
     e2e_value, h2d = None, 0
     if e2e_steps > 0:
@@ -398,6 +423,7 @@ def run_ours(args):
                      "share_of_kernel_time": d["ms"] / max(1e-9, sum(v["ms"] for v in kt.values()))},
         "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
         "gpu_launches": n_launch,
+        "mixed": mixed,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

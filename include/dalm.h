@@ -104,14 +104,17 @@ typedef struct {
                              cell order instead of a parallel tree; with it
                              the FP64 step reproduces the reference's
                              rounding (slow: for parity checks)          */
-    int fused_krylov;     /* 1 (default): each half of a Jacobi(3)-
-                             BiCGStab iteration (update, preconditioner,
-                             SpMV, dot products) as one kernel; 0: one
-                             kernel per reference loop.  Ignored with
-                             reference_sums and other preconditioners.  */
+    int fused_krylov;     /* 1: each half of a Jacobi(3)-BiCGStab
+                             iteration (update, preconditioner, SpMV, dot
+                             products) as one kernel, 20 instead of 35
+                             vectors per cell per iteration; 0 (default):
+                             one kernel per reference loop, which is as
+                             fast on B200 today (the fused kernels are
+                             latency-bound).  Ignored with reference_sums
+                             and other preconditioners.                 */
     int refine_inner_it;  /* DALM_MIXED: FP32 iterations per refinement
                              pass before the FP64 residual is recomputed
-                             (0: automatic, 50)                          */
+                             (0: automatic, 100)                         */
     int reserved[5];
 } dalm_options;
 

@@ -90,7 +90,7 @@ def test_fused_within_envelope_of_oracle(make_case, n):
 def test_fused_iteration_cap_and_kernels(make_case):
     pkg = package()
     spec, mesh, d, U0, prof = make_case("tiny-loglaw", n=GRIDS[0])
-    s = pkg.Solver(d, profile=True)
+    s = pkg.Solver(d, profile=True, fused_krylov=True)
     s.set_inflow_profile(prof)
     s.set_state(U0)
     s.set_poisson(7, 0.0)
