@@ -29,6 +29,8 @@ constexpr double PI_D = 3.14159265358979323846;
 // Truncation radius of the Gaussian projection: r^2 <= 40 eps^2, where the
 // dropped weight exp(-40) ~ 4e-18 of the peak is below FP64 resolution of f.
 constexpr double ALM_CUTOFF_EPS2 = 40.0;
+// iterations per captured CUDA graph of the Poisson loop
+constexpr int GRAPH_UNIT = 8;
 // Iterative refinement (DALM_MIXED): an FP32 inner solve stops at
 // INNER_RTOL x the FP64 residual or after the pass cap (refine_inner_it,
 // default INNER_CAP iterations); a pass that shrinks the FP64 residual by
@@ -97,6 +99,10 @@ struct dalm_handle {
     double *partial = nullptr;
     unsigned int *ticket = nullptr;
     KrylovState *d_kst = nullptr, *h_kst = nullptr;
+    struct GraphUnit {
+        cudaGraphExec_t exec = nullptr;
+        long long kernels = 0;
+    } graph_unit[2];  // per solve (FP64, FP32 inner)
     bool trace = false;          // DALM_TRACE_POISSON=1: one stderr line per pressure solve
     bool trace_batches = false;  // DALM_TRACE_POISSON=2: also one per batch of iterations
     DiagState *d_diag = nullptr, *h_diag = nullptr;
@@ -125,6 +131,10 @@ struct dalm_handle {
 
     void release() {
         if (stream) cudaStreamSynchronize(stream);
+        for (auto &gu : graph_unit) {
+            if (gu.exec) cudaGraphExecDestroy(gu.exec);
+            gu.exec = nullptr;
+        }
         for (void *p : allocs) cudaFree(p);
         allocs.clear();
         if (h_kst) cudaFreeHost(h_kst);
@@ -474,19 +484,60 @@ struct dalm_handle {
     // `hint` (the previous comparable solve's count); later batches grow
     // with the count so far.  Kernels enqueued after convergence return at
     // once.  Returns the iterations the solve took.
+    // one iteration n of solve `which` (0: the FP64 solve, 1: the FP32
+    // inner solve of the mixed form)
+    void enqueue_one(int which, long long n, KrylovState *st) {
+        if (which == 1)
+            launch_bicg_iteration<float>(L, g, coef, pbf, pcfg, Partials<2>{partial, ticket}, st);
+        else
+            enqueue_poisson_iteration(n);
+    }
+    // CUDA graphs (opt.use_graphs, not with per-kernel profiling): a unit of
+    // GRAPH_UNIT iterations of a solve is captured once per handle and
+    // replayed.  Kernel arguments are fixed per handle (the Krylov scalars
+    // live in device memory); the fused kernels' ping-pong depends only on
+    // the iteration's parity, and units start at even iterations.
+    bool use_graphs() const { return opt.use_graphs && !opt.profile; }
+    void enqueue_unit(int which, long long n0) {
+        GraphUnit &gu = graph_unit[which];
+        if (!gu.exec) {
+            const long long before = launch_count;
+            cudaGraph_t graph = nullptr;
+            DALM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                for (int n = 0; n < GRAPH_UNIT; n++) enqueue_one(which, n0 + n, d_kst + which);
+            } catch (...) {
+                cudaStreamEndCapture(stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                launch_count = before;
+                throw;
+            }
+            DALM_CUDA(cudaStreamEndCapture(stream, &graph));
+            cudaError_t e = cudaGraphInstantiate(&gu.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            DALM_CUDA(e);
+            gu.kernels = launch_count - before;
+            launch_count = before;  // capturing launched nothing
+        }
+        DALM_CUDA(cudaGraphLaunch(gu.exec, stream));
+        launch_count += gu.kernels;
+    }
     long long run_batches(int which, long long hint, long long cap) {
         KrylovState *st = d_kst + which;
         long long issued = 0;
         long long batch = opt.poisson_batch > 0
                               ? opt.poisson_batch
                               : std::min<long long>(256, hint > 12 ? hint / 2 : 4);
+        const bool graphs = use_graphs();
         while (true) {
             batch = std::min<long long>(batch, std::max<long long>(1, cap - issued));
-            for (long long n = 0; n < batch; n++) {
-                if (which == 1)
-                    launch_bicg_iteration<float>(L, g, coef, pbf, pcfg, Partials<2>{partial, ticket}, st);
-                else
-                    enqueue_poisson_iteration(issued + n);
+            if (graphs) {
+                // whole units; iterations past the stop return at once
+                const long long units = (batch + GRAPH_UNIT - 1) / GRAPH_UNIT;
+                for (long long u = 0; u < units; u++) enqueue_unit(which, issued + u * GRAPH_UNIT);
+                batch = units * GRAPH_UNIT;
+            } else {
+                for (long long n = 0; n < batch; n++) enqueue_one(which, issued + n, st);
             }
             issued += batch;
             fetch_states();
@@ -494,7 +545,7 @@ struct dalm_handle {
                 std::fprintf(stderr, "[dalm]     solve %d: %lld iterations, residual %.3e\n", which,
                              (long long)h_kst[which].it, h_kst[which].err);
             if (h_kst[which].done) break;
-            if (issued > cap + 1)
+            if (issued > cap + GRAPH_UNIT)
                 throw std::runtime_error("Poisson loop did not stop at its iteration limit");
             batch = opt.poisson_batch > 0 ? opt.poisson_batch
                                           : std::max<long long>(8, std::min<long long>(96, issued / 8));
