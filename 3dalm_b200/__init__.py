@@ -54,7 +54,8 @@ class Options(C.Structure):
                 ("time_average", C.c_int), ("check_finite", C.c_int),
                 ("poisson_batch", C.c_int), ("use_graphs", C.c_int), ("profile", C.c_int),
                 ("reference_sums", C.c_int), ("fused_krylov", C.c_int),
-                ("refine_inner_it", C.c_int), ("reserved", C.c_int * 5)]
+                ("refine_inner_it", C.c_int), ("write_output", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 _PD = C.POINTER(C.c_double)
@@ -96,7 +97,7 @@ class Solver:
     def __init__(self, case_dir: str | None = None, precision: int = FP64, device: int = 0,
                  time_average: bool = True, profile: bool = False, poisson_batch: int = 0,
                  limiter: int = MINMOD, reference_sums: bool = False, fused_krylov: bool = False,
-                 refine_inner_it: int = 0):
+                 refine_inner_it: int = 0, write_output: bool = False):
         self.lib = load_library()
         self.h = C.c_void_p()
         self.opt = Options()
@@ -110,6 +111,7 @@ class Solver:
         self.opt.reference_sums = int(reference_sums)
         self.opt.fused_krylov = int(fused_krylov)
         self.opt.refine_inner_it = int(refine_inner_it)
+        self.opt.write_output = int(write_output)
         if case_dir is not None:
             self.initialize(case_dir)
 

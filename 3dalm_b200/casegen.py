@@ -173,6 +173,8 @@ class CaseSpec:
     seed: int = 0
     loglaw: tuple | None = None     # (u_star, z0)
     tavg_start_time: float = 1e30
+    output_start_time: float = 1e30
+    output_interval_time: float = 1e30
     polar_step_deg: float = 0.5
 
 
@@ -235,7 +237,8 @@ def setup_json(spec: CaseSpec, mesh: Mesh) -> dict:
         eq["preconditioner"] = pc
     js = {
         "runtime": {"dt": spec.dt, "time": spec.steps * spec.dt},
-        "output": {"output start time": 1e30, "output interval time": 1e30,
+        "output": {"output start time": spec.output_start_time,
+                   "output interval time": spec.output_interval_time,
                    "time avg start time": spec.tavg_start_time},
         "inflow": {"value": list(spec.uin)},
         "cfd": {"Re": spec.re, "Cs": spec.cs},

@@ -119,6 +119,8 @@ CaseData load_case(const std::string &dir) {
     double total_time = setup["runtime"]["time"].number();
     c.max_step = (int64_t)(total_time / c.dt);
     c.tavg_start_time = setup["output"]["time avg start time"].number();
+    c.output_start_time = setup["output"]["output start time"].number();
+    c.output_interval_time = setup["output"]["output interval time"].number();
     if (setup.contains("turbulence grid"))
         throw std::runtime_error("setup.json: \"turbulence grid\" is not supported by this build");
     if (setup.contains("floor start"))

@@ -27,6 +27,7 @@ struct CaseData {
     double re = 0, cs = 0, dt = 0;
     int64_t max_step = 0;
     double tavg_start_time = 0;
+    double output_start_time = 0, output_interval_time = 0;
     std::string method, pc_method;  // "SOR" | "BiCG" | "Jacobi"; "Jacobi" | "SOR"
     int64_t max_it = 0, pc_max_it = 0;
     double tol = 0, relax = 1, pc_relax = 1;

@@ -10,6 +10,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <filesystem>
+#include <fstream>
 #include <memory>
 #include <string>
 #include <vector>
@@ -17,6 +19,7 @@
 #include "../../include/dalm.h"
 #include "alm.cuh"
 #include "case_io.hpp"
+#include "output_io.hpp"
 #include "poisson.cuh"
 
 using namespace dalm;
@@ -103,6 +106,11 @@ struct dalm_handle {
         cudaGraphExec_t exec = nullptr;
         long long kernels = 0;
     } graph_unit[2];  // per solve (FP64, FP32 inner)
+    // output in the reference's formats (opt.write_output)
+    std::string out_dir;
+    double next_output_time = 0;
+    std::vector<SnapshotEntry> snapshots;
+    std::ofstream turbine_log;
     bool trace = false;          // DALM_TRACE_POISSON=1: one stderr line per pressure solve
     bool trace_batches = false;  // DALM_TRACE_POISSON=2: also one per batch of iterations
     DiagState *d_diag = nullptr, *h_diag = nullptr;
@@ -342,6 +350,7 @@ struct dalm_handle {
             for (int m = 0; m < 3; m++) launch_fill(L, U[b][m], g.total, cs.uin[m]);
         refresh_after_state(DALM_SET_APPLY_UBC | DALM_SET_RECOMPUTE_JU, nullptr);
         DALM_CUDA(cudaStreamSynchronize(stream));
+        if (opt.write_output) init_output();
     }
 
     // (Cs * cbrt(dx dy dz))^2 per interior cell with the host libm's cbrt,
@@ -743,7 +752,70 @@ struct dalm_handle {
             stage_alm();
         }
         stage_tavg();
+        if (opt.write_output) write_outputs();
         step++;
+    }
+
+    // ---- output in the reference's formats -------------------------------
+    // output/ beside the case files like the reference's solver
+    // (src/solver.h:569-588), partition.json (src/solver.h:980-998), and a
+    // per-turbine load time series turbines.csv (no reference counterpart).
+    void init_output() {
+        out_dir = (std::filesystem::path(cs.dir) / "output").string();
+        std::filesystem::create_directories(out_dir);
+        write_partition_json(out_dir + "/partition.json", cs.size, cs.gc);
+        next_output_time = cs.output_start_time;
+        if (alm.wt_count > 0) {
+            turbine_log.open(out_dir + "/turbines.csv");
+            if (!turbine_log) throw std::runtime_error("cannot write " + out_dir + "/turbines.csv");
+            turbine_log << "step,time";
+            for (int w = 0; w < alm.wt_count; w++)
+                turbine_log << ",thrust" << w << ",torque" << w << ",power" << w;
+            turbine_log << "\n";
+        }
+    }
+    // The end of main_loop_once (src/solver.h:1194-1253): the turbine loads,
+    // and at the output times the inst_ file (U, p, div, q, f), the tavg_
+    // file (time-averaged U) once averaging has started, and snapshot.json.
+    void write_outputs() {
+        const double t = cs.dt * (double)step;
+        if (turbine_log.is_open() && step != 0) {
+            sync_stats();
+            char buf[96];
+            std::snprintf(buf, sizeof buf, "%lld,%.17g", (long long)step, t);
+            turbine_log << buf;
+            for (int w = 0; w < alm.wt_count; w++) {
+                const double tq = h_wt_out[w], th = h_wt_out[alm.wt_count + w];
+                std::snprintf(buf, sizeof buf, ",%.17g,%.17g,%.17g", th, tq,
+                              tq * std::fabs(h_wt[w].rot_speed));
+                turbine_log << buf;
+            }
+            turbine_log << "\n";
+            turbine_log.flush();
+        }
+        if (!(t - 0.5 * cs.dt < next_output_time && next_output_time <= t + 0.5 * cs.dt)) return;
+        next_output_time += cs.output_interval_time;
+        const size_t cells = (size_t)g.nx * g.ny * g.nz;
+        std::vector<double> u(3 * cells), p(cells), dv(cells), q(cells), f(3 * cells);
+        get_field(DALM_FIELD_U, u.data());
+        get_field(DALM_FIELD_P, p.data());
+        get_field(DALM_FIELD_DIV, dv.data());
+        double *s = scratch_field();
+        launch_q_field(L, P, c(u_cur()), s);
+        download_field(&s, 1, q.data());
+        get_field(DALM_FIELD_F, f.data());
+        write_field_binary(out_dir + "/" + binary_filename("inst", 0, step), cs.size, cs.gc, cs.x,
+                           cs.y, cs.z,
+                           {{"U", 3, u.data()}, {"p", 1, p.data()}, {"div", 1, dv.data()},
+                            {"q", 1, q.data()}, {"f", 3, f.data()}});
+        const bool tavg = t >= cs.tavg_start_time;
+        if (tavg) {
+            get_field(DALM_FIELD_UTAVG, u.data());
+            write_field_binary(out_dir + "/" + binary_filename("tavg", 0, step), cs.size, cs.gc,
+                               cs.x, cs.y, cs.z, {{"U", 3, u.data()}});
+        }
+        snapshots.push_back({step, t, tavg});
+        write_snapshot_json(out_dir + "/snapshot.json", snapshots);
     }
 
     // derived quantities after a state change (src/solver.h:767-833)
@@ -883,6 +955,7 @@ void dalm_default_options(dalm_options *opt) {
     opt->profile = 0;
     opt->reference_sums = 0;
     opt->fused_krylov = 0;
+    opt->write_output = 0;
     opt->refine_inner_it = 0;
 }
 

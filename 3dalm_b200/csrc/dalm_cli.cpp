@@ -1,8 +1,10 @@
-// Command-line driver: `dalm <case_dir> [--steps N] [--quiet]`.
+// Command-line driver:
+//   dalm <case_dir> [--steps N] [--quiet] [--no-output] [--reference-sums] [--mixed]
 // Mirrors the reference's `solver <case_dir>` (src/solver.cpp:6-47): runs
-// steps 0..max_step (or N steps) and prints the per-step line
-// `step time it err avg_div max_cfl` (src/solver.h:1188-1190), then the
-// per-turbine thrust, torque and power.
+// steps 0..max_step (or N steps), prints the per-step line
+// `step time it err avg_div max_cfl` (src/solver.h:1188-1190), writes the
+// reference's output files into <case_dir>/output (unless --no-output), then
+// prints the per-turbine thrust, torque and power.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -28,7 +30,10 @@ static bool read_raw(const std::string &path, std::vector<double> &v) {
 
 int main(int argc, char **argv) {
     if (argc < 2) {
-        fprintf(stderr, "usage: %s <case_dir> [--steps N] [--quiet]\n", argv[0]);
+        fprintf(stderr,
+                "usage: %s <case_dir> [--steps N] [--quiet] [--no-output] [--reference-sums] "
+                "[--mixed]\n",
+                argv[0]);
         return 2;
     }
     const char *dir = argv[1];
@@ -36,9 +41,17 @@ int main(int argc, char **argv) {
     bool quiet = false;
     dalm_options opt;
     dalm_default_options(&opt);
+    opt.write_output = 1;
     for (int a = 2; a < argc; a++) {
         if (!strcmp(argv[a], "--steps") && a + 1 < argc) steps = atoll(argv[++a]);
         else if (!strcmp(argv[a], "--quiet")) quiet = true;
+        else if (!strcmp(argv[a], "--no-output")) opt.write_output = 0;
+        else if (!strcmp(argv[a], "--reference-sums")) opt.reference_sums = 1;
+        else if (!strcmp(argv[a], "--mixed")) opt.precision = DALM_MIXED;
+        else {
+            fprintf(stderr, "unknown option %s\n", argv[a]);
+            return 2;
+        }
     }
     time_t t0 = time(0);
     printf("START %s\n", ctime(&t0));

@@ -99,6 +99,8 @@ void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                  Vec3<const double> ju, Partials<2> part, DiagState *diag);
 void launch_nut_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> u, double *nut);
 void launch_div_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> ju, double *div);
+// Q-criterion of U on the interior (calc_q, src/cfd.h:949-1034)
+void launch_q_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> u, double *q);
 void launch_tavg(const LaunchCtx &L, const Grid &g, Vec3<double> tavg, Vec3<const double> u,
                  double w);
 // reference AoS/scalar layout <-> device SoA layout (ncomp = 1 or 3)

@@ -497,6 +497,35 @@ k_div_field(StepParams P, Tiling T, Vec3<const double> JU, double *div) {
     }
 }
 
+// Q-criterion on the interior (calc_q_at_cell, src/cfd.h:949-975): central
+// differences over x[i+1] - x[i-1] etc., same operation order.
+__global__ void __launch_bounds__(TILE_THREADS)
+k_q_field(StepParams P, Tiling T, Vec3<const double> U, double *q) {
+    const Grid &g = P.g;
+    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
+        int i, j, k;
+        if (!T.cell(tile, i, j, k)) continue;
+        const long long c = g.at(i, j, k);
+        const long long ce = g.at(i + 1, j, k), cw = g.at(i - 1, j, k);
+        const long long cn = g.at(i, j + 1, k), cs = g.at(i, j - 1, k);
+        const long long ct = c + 1, cb = c - 1;
+        const double dxew = P.m.x[i + 1] - P.m.x[i - 1];
+        const double dyns = P.m.y[j + 1] - P.m.y[j - 1];
+        const double dztb = P.m.z[k + 1] - P.m.z[k - 1];
+        const double dudx = (U.c[0][ce] - U.c[0][cw]) / dxew;
+        const double dudy = (U.c[0][cn] - U.c[0][cs]) / dyns;
+        const double dudz = (U.c[0][ct] - U.c[0][cb]) / dztb;
+        const double dvdx = (U.c[1][ce] - U.c[1][cw]) / dxew;
+        const double dvdy = (U.c[1][cn] - U.c[1][cs]) / dyns;
+        const double dvdz = (U.c[1][ct] - U.c[1][cb]) / dztb;
+        const double dwdx = (U.c[2][ce] - U.c[2][cw]) / dxew;
+        const double dwdy = (U.c[2][cn] - U.c[2][cs]) / dyns;
+        const double dwdz = (U.c[2][ct] - U.c[2][cb]) / dztb;
+        q[c] = -0.5 * (dudx * dudx + dvdy * dvdy + dwdz * dwdz +
+                       2 * (dudy * dvdx + dudz * dwdx + dvdz * dwdy));
+    }
+}
+
 // Running time average over every stored cell (calc_ax_plus_by,
 // src/mv.h:322-335 as used at src/solver.h:1198-1203).
 __global__ void k_tavg(Grid g, Vec3<double> A, Vec3<const double> U, double w) {
@@ -645,6 +674,13 @@ void launch_div_field(const LaunchCtx &L, const StepParams &P, Vec3<const double
     Tiling T = Tiling::make(interior_box(P.g));
     L.pre(KK_LAYOUT);
     k_div_field<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, ju, div);
+    L.post(KK_LAYOUT);
+}
+
+void launch_q_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> u, double *q) {
+    Tiling T = Tiling::make(interior_box(P.g));
+    L.pre(KK_LAYOUT);
+    k_q_field<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, q);
     L.post(KK_LAYOUT);
 }
 

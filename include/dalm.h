@@ -115,7 +115,12 @@ typedef struct {
     int refine_inner_it;  /* DALM_MIXED: FP32 iterations per refinement
                              pass before the FP64 residual is recomputed
                              (0: automatic, 100)                         */
-    int reserved[5];
+    int write_output;     /* 1: dalm_step writes the reference's output
+                             files into <case_dir>/output at the case's
+                             output times (inst_/tavg_ binaries with U, p,
+                             div, q, f / U, snapshot.json, partition.json)
+                             and a per-turbine turbines.csv every step   */
+    int reserved[4];
 } dalm_options;
 
 /* Fills *opt with the defaults (FP64, minmod, device 0, time average on,
