@@ -100,6 +100,24 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(v, world):
+    """The largest of every rank's v (the job's time is its slowest replica's)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(cells, steps, world, seconds):
+    """Mcell-steps/s of the whole job: every rank advances its own replica of
+    `cells` cells by `steps` steps (weak scaling) in `seconds` (max over ranks)."""
+    return cells * steps * world / seconds / 1e6
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -324,21 +342,18 @@ def run_ours(args):
         clk = clocks.stop()
         ms = e0.elapsed_time(e1)
         _, launches = s.timings()
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, world)
         s.finalize()
         return ms, its, errs, clk, launches
 
     # ---- the reference's precision: the headline
     ms, its, errs, clk, launches = timed_region(pkg.FP64)
-    value = n_int * args.steps * world / (ms / 1e3) / 1e6
+    value = whole_job_rate(n_int, args.steps, world, ms / 1e3)
     # ---- the mixed-precision form on the same steps
     mixed = None
     if not args.no_mixed:
         mms, mits, merrs, mclk, _ = timed_region(pkg.MIXED)
-        mvalue = n_int * args.steps * world / (mms / 1e3) / 1e6
+        mvalue = whole_job_rate(n_int, args.steps, world, mms / 1e3)
         mixed = {"value": mvalue, "unit": METRIC, "ms_per_step": mms / args.steps,
                  "vs_fp64": mvalue / value, "poisson_iterations": mits,
                  "max_residual": max(merrs), "fp64_max_residual": max(errs),
@@ -374,11 +389,8 @@ def run_ours(args):
         if e2e_its != its[:e2e_steps]:
             raise RuntimeError(f"end-to-end replay took other iteration counts {e2e_its} "
                                f"than the timed region {its[:e2e_steps]}")
-        if world > 1:
-            t = torch.tensor([e2e_s], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e_value = n_int * e2e_steps * world / e2e_s / 1e6
+        e2e_s = max_over_ranks(e2e_s, world)
+        e2e_value = whole_job_rate(n_int, e2e_steps, world, e2e_s)
         h2d = U_h.nbytes + p_h.nbytes
         s.finalize()
 
