@@ -38,7 +38,7 @@ constexpr int WJ = TJ + 2 * WIDE_HJ;      // 14: j0 - 3 .. j0 + 10
 constexpr int WN = WK * WJ;               // doubles per plane buffer
 constexpr int PB = WN * 8;                // bytes per plane buffer
 constexpr int TB = TK * TJ * 8;           // bytes per tile plane (r0)
-constexpr int NSF = 3;                    // TMA ring depth
+constexpr int NSF = 4;                    // TMA ring depth
 constexpr int MAXP = 32 + 2 * FH;         // planes a block loads at most (chunks <= 32)
 constexpr int NRING_A = 84, NRING_B = 92, NRING_C = 128;  // halo rings, see ring_cell
 constexpr int NEXTRA = NRING_A + NRING_B + NRING_C - TILE_THREADS;  // second ring cells: 48
@@ -49,7 +49,8 @@ template <int KIND>
 struct FusedGeo {
     static constexpr int NIN = KIND == FK_P ? 3 : 2;   // wide inputs per plane
     static constexpr int STAGE = NIN * PB + (KIND == FK_P ? TB : 0);
-    static constexpr int SMEM = NSF * STAGE + 3 * 2 * PB;  // + w1, w2, w3 planes, two each
+    // + w1, w2, w3 planes (two each) and 1/ac planes (three)
+    static constexpr int SMEM = NSF * STAGE + (3 * 2 + 3) * PB;
 };
 
 struct FusedArgs {
@@ -186,16 +187,19 @@ k_fused(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m
     auto W1s = [&](int m) { return wpl + (0 + (m & 1)) * WN; };
     auto W2s = [&](int m) { return wpl + (2 + (m & 1)) * WN; };
     auto W3s = [&](int m) { return wpl + (4 + (m & 1)) * WN; };
+    auto Rs = [&](int m) { return wpl + (6 + m % 3) * WN; };   // 1/ac, computed in phase 1
 
-    // phase 1 at one owned cell: v and w1 = v / ac (the first sweep from zero)
+    // phase 1 at one owned cell: v, 1/ac and w1 = v / ac (the first sweep
+    // from zero)
     auto point = [&](const OwnCell &o, const double *in_a, const double *in_b, const double *in_c,
-                     bool pin, double xp, double &v, double &w) {
+                     bool pin, double xp, double &v, double &w, double &rc) {
         const int e = o.idx;
         if (KIND == FK_P)
             v = first ? in_a[e] : __fma_rn(beta, __fma_rn(-omega, in_c[e], in_b[e]), in_a[e]);
         else
             v = __fma_rn(-alpha, in_c[e], in_a[e]);
-        w = v * fast_rcp((xp - o.cs) * inv_md);
+        rc = fast_rcp((xp - o.cs) * inv_md);
+        w = v * rc;
         const bool in = pin && o.in;
         v = in ? v : 0.0;
         w = in ? w : 0.0;
@@ -213,12 +217,13 @@ k_fused(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m
         v = __fma_rn(o.at, P[o.idx + 1], v);
         return __fma_rn(o.ab, P[o.idx - 1], v);
     };
-    // sweep_jacobi_at_cell (relax<false>) at an owned cell of plane m
+    // sweep_jacobi_at_cell (relax<false>) at an owned cell of plane m; 1/ac
+    // from the plane's ring (the same fast_rcp value phase 1 computed)
     auto sweep = [&](const OwnCell &o, const double *P, int m, bool pin, double xc, double xe,
                      double xw, double rhs) {
         const double ac = (s_xp[m] - o.cs) * inv_md;
         const double ax = ax_at(o, P, m, ac, xc, xe, xw);
-        const double w = xc + (rhs - ax) * fast_rcp(ac);
+        const double w = xc + (rhs - ax) * Rs(m)[o.idx];
         return (pin && o.in) ? w : 0.0;
     };
 
@@ -242,8 +247,11 @@ k_fused(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m
         rv2 = rv1; rv1 = rv0;
         r12 = r11; r11 = r10;
         r22 = r21; r21 = r20;
+        // Three barriers per step (after phases 1, 2 and 3): phase 4 of step
+        // L and phase 1 of step L + 1 touch disjoint buffers (W3 / stage L
+        // against W1, 1/ac and stage L + 1), and a failed wait is caught at
+        // the first barrier, before any shared plane it touched is read.
         if (!fail) fail = !mbar_wait(&bar[L % NSF], (unsigned)((L / NSF) & 1));
-        if (__syncthreads_or(fail)) break;
         const unsigned char *stg = smem + (L % NSF) * G::STAGE;
         const double *in_a = (const double *)stg;
         const double *in_b = (const double *)(stg + PB);
@@ -253,17 +261,28 @@ k_fused(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m
         {   // phase 1, plane L
             const bool pin = plane_in(L);
             const double xp = s_xp[L];
-            double *P1 = W1s(L);
-            double xv = 0.0, xw = 0.0;
-            point(cT, in_a, in_b, in_c, pin, xp, tv0, t10);
-            point(cR, in_a, in_b, in_c, pin, xp, rv0, r10);
-            if (has_x) point(cX, in_a, in_b, in_c, pin, xp, xv, xw);
+            double *P1 = W1s(L), *R1 = Rs(L);
+            double xv = 0.0, xw = 0.0, rc_t = 0.0, rc_r = 0.0, rc_x = 0.0;
+            point(cT, in_a, in_b, in_c, pin, xp, tv0, t10, rc_t);
+            point(cR, in_a, in_b, in_c, pin, xp, rv0, r10, rc_r);
+            if (has_x) point(cX, in_a, in_b, in_c, pin, xp, xv, xw, rc_x);
             P1[cT.idx] = t10;
             P1[cR.idx] = r10;
-            if (has_x) P1[cX.idx] = xw;
-            if (cT.in && L >= FH && L < FH + np) A.v_out[(long long)(ib + L) * g.sx + toff] = tv0;
+            R1[cT.idx] = rc_t;
+            R1[cR.idx] = rc_r;
+            if (has_x) {
+                P1[cX.idx] = xw;
+                R1[cX.idx] = rc_x;
+            }
+            if (!fail && cT.in && L >= FH && L < FH + np)
+                A.v_out[(long long)(ib + L) * g.sx + toff] = tv0;
         }
-        __syncthreads();
+        if (__syncthreads_or(fail)) break;
+        // every thread is past step L - 1: its stage is free for load L - 1 + NSF
+        if (tid == 0 && L >= 1 && issued < nload) {
+            fence_proxy_async();  // the released stage was read through the generic proxy
+            issue(issued++);
+        }
         if (L >= 2) {   // phase 2, plane L - 1
             const int m = L - 1;
             const bool pin = plane_in(m);
@@ -300,11 +319,6 @@ k_fused(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m
                 acc0 += ax * tv3;
                 acc1 += ax * ax;
             }
-        }
-        __syncthreads();
-        if (tid == 0 && issued < nload) {
-            fence_proxy_async();  // the released stage was read through the generic proxy
-            issue(issued++);
         }
     }
     if (fail) {
