@@ -118,6 +118,10 @@ struct Segments {
     Box box;
     int ntk, ntj, ncol, nchunk, ich;
     int count;
+    // Enough segments to fill the GPU, chunks of at most 32 planes.  (Sizing
+    // the chunk count to fill whole waves of resident blocks was measured
+    // slower on the 512x256x128 case: shorter chunks cost more than the
+    // last wave's idle slots.)
     __host__ static Segments make(const Box &b, int target_blocks) {
         Segments s;
         s.box = b;
@@ -139,14 +143,19 @@ struct Segments {
         s.count = s.ncol * s.nchunk;
         return s;
     }
+    // planes [i0, i1) of a chunk: balanced, at most ich planes
+    __host__ __device__ void chunk_range(int chunk, int &i0, int &i1) const {
+        const long long ni = box.hi[0] - box.lo[0];
+        i0 = box.lo[0] + (int)(chunk * ni / nchunk);
+        i1 = box.lo[0] + (int)((chunk + 1) * ni / nchunk);
+    }
     // this thread's (k, j) and the segment's [i0, i1); false when (k, j) is
     // outside the box
     __device__ bool column(int u, int &i0, int &i1, int &j, int &k) const {
         int col = u % ncol, chunk = u / ncol;
         k = box.lo[2] + (col % ntk) * TK + (int)(threadIdx.x & 31);
         j = box.lo[1] + (col / ntk) * TJ + (int)(threadIdx.x >> 5);
-        i0 = box.lo[0] + chunk * ich;
-        i1 = min(i0 + ich, box.hi[0]);
+        chunk_range(chunk, i0, i1);
         return k < box.hi[2] && j < box.hi[1];
     }
 };

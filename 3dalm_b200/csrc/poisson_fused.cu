@@ -118,7 +118,8 @@ k_fused(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m
     const int u = blockIdx.x;
     const int col = u % S.ncol, chunk = u / S.ncol;
     const int k0 = S.box.lo[2] + (col % S.ntk) * TK, j0 = S.box.lo[1] + (col / S.ntk) * TJ;
-    const int i0 = S.box.lo[0] + chunk * S.ich, i1 = min(i0 + S.ich, S.box.hi[0]);
+    int i0, i1;
+    S.chunk_range(chunk, i0, i1);
     const int np = i1 - i0, nload = np + 2 * FH;
     const int kb = k0 - WIDE_HK, jb = j0 - WIDE_HJ, ib = i0 - FH;
     const int off = (int)g.off;
