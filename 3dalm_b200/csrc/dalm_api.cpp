@@ -240,9 +240,8 @@ struct dalm_handle {
         opt = o;
         if (opt.precision != DALM_FP64 && opt.precision != DALM_MIXED)
             throw std::invalid_argument("unknown precision");
-        if (opt.limiter == DALM_LIMITER_VAN_ALBADA)
-            throw Unsupported("the van Albada limiter is not implemented in this build");
-        if (opt.limiter != DALM_LIMITER_MINMOD) throw std::invalid_argument("unknown limiter");
+        if (opt.limiter != DALM_LIMITER_MINMOD && opt.limiter != DALM_LIMITER_VAN_ALBADA)
+            throw std::invalid_argument("unknown limiter");
         const char *tr = std::getenv("DALM_TRACE_POISSON");
         trace = tr && (tr[0] == '1' || tr[0] == '2');
         trace_batches = tr && tr[0] == '2';
@@ -340,6 +339,7 @@ struct dalm_handle {
         P.prof = nullptr;
         P.fbox = fbox;
         P.reference_sums = opt.reference_sums ? 1 : 0;
+        P.limiter = opt.limiter == DALM_LIMITER_VAN_ALBADA ? 1 : 0;
         P.filter2 = build_filter();
 
         init_alm();

@@ -43,6 +43,7 @@ struct StepParams {
     // 1: global sums in the reference's serial (i,j,k) order
     // (warp_serial_sums) instead of the parallel tree
     int reference_sums;
+    int limiter;  // 0: the reference's b=4 limiter, 1: van Albada
 };
 
 struct DiagState {

@@ -12,15 +12,36 @@ namespace {
 
 __device__ __forceinline__ double sgn(double v) { return (double)((v > 0.) - (v < 0.)); }
 
+// The smooth van Albada limiter (DALM_LIMITER_VAN_ALBADA, an extension: the
+// reference has only the limiter above): the face value of a cell with
+// backward / forward differences a, b is  f +- (s/4)[(1 - k s) a + (1 + k s) b]
+// with the switch s = (2ab + eps)/(a^2 + b^2 + eps) (van Albada, van Leer &
+// Roberts 1982, in the kappa-MUSCL form), eps = 1e-12; differentiable
+// everywhere, unlike the b=4 limiter.
+__device__ __forceinline__ double va_switch(double a, double b) {
+    const double eps = 1e-12;
+    return (2. * a * b + eps) / (a * a + b * b + eps);
+}
+
 // κ=1/3 MUSCL reconstruction with the b=(3-κ)/(1-κ) limiter and the upwind
 // face flux along one axis (src/cfd.h:37-60): returns flux(+) - flux(-).
 __device__ __forceinline__ void muscl_axis(double fmm, double fm, double fc, double fp,
                                            double fpp, double Jp, double Jm, double &flux_p,
-                                           double &flux_m) {
+                                           double &flux_m, int limiter) {
     const double kap = 1. / 3.;
     const double bb = (3. - kap) / (1. - kap);
     const double e = 1.;
     double d4 = fpp - fp, d3 = fp - fc, d2 = fc - fm, d1 = fm - fmm;
+    if (limiter == 1) {
+        const double sp = va_switch(d4, d3), sc = va_switch(d3, d2), sm = va_switch(d2, d1);
+        const double fpr = fp - (sp / 4.) * ((1. - kap * sp) * d4 + (1. + kap * sp) * d3);
+        const double fpl = fc + (sc / 4.) * ((1. - kap * sc) * d2 + (1. + kap * sc) * d3);
+        const double fmr = fc - (sc / 4.) * ((1. - kap * sc) * d3 + (1. + kap * sc) * d2);
+        const double fml = fm + (sm / 4.) * ((1. - kap * sm) * d1 + (1. + kap * sm) * d2);
+        flux_p = 0.5 * (Jp * (fpr + fpl) - fabs(Jp) * (fpr - fpl));
+        flux_m = 0.5 * (Jm * (fmr + fml) - fabs(Jm) * (fmr - fml));
+        return;
+    }
     double s4 = sgn(d4), s3 = sgn(d3), s2 = sgn(d2), s1 = sgn(d1);
     double g6 = s4 * fmax(0., fmin(fabs(d4), s4 * bb * d3));
     double g5 = s3 * fmax(0., fmin(fabs(d3), s3 * bb * d4));
@@ -111,9 +132,9 @@ k_predict(StepParams P, Tiling T, Vec3<const double> V, Vec3<double> Un, Vec3<co
             const double *v = V.c[m];
             double fc = v[c];
             double fE, fW, fN, fS, fT, fB;
-            muscl_axis(v[ww], v[w], fc, v[e], v[ee], JUE, JUW, fE, fW);
-            muscl_axis(v[ss], v[s], fc, v[n], v[nn], JVN, JVS, fN, fS);
-            muscl_axis(v[bb], v[b], fc, v[t], v[tt], JWT, JWB, fT, fB);
+            muscl_axis(v[ww], v[w], fc, v[e], v[ee], JUE, JUW, fE, fW, P.limiter);
+            muscl_axis(v[ss], v[s], fc, v[n], v[nn], JVN, JVS, fN, fS, P.limiter);
+            muscl_axis(v[bb], v[b], fc, v[t], v[tt], JWT, JWB, fT, fB, P.limiter);
             double conv = (fE - fW + fN - fS + fT - fB) / J;
             double diff = visc * (((v[e] - fc) / (xe - xi) - (fc - v[w]) / (xi - xw)) / dxc +
                                   ((v[n] - fc) / (yn - yj) - (fc - v[s]) / (yj - ys)) / dyc +

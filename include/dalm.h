@@ -53,8 +53,9 @@ enum dalm_precision {
 enum dalm_limiter {
     DALM_LIMITER_MINMOD = 0,    /* the reference's b=4 minmod-type limiter,
                                    src/cfd.h:37-54                           */
-    DALM_LIMITER_VAN_ALBADA = 1 /* reserved for a smooth limiter (not in the
-                                   reference): DALM_ERR_UNSUPPORTED       */
+    DALM_LIMITER_VAN_ALBADA = 1 /* smooth van Albada limiter (extension: not in
+                                   the reference), kappa-MUSCL form:
+                                   s = (2ab+eps)/(a^2+b^2+eps), eps 1e-12  */
 };
 
 /* Fields addressable by dalm_get_field / dalm_set_field (reference arrays). */

@@ -45,6 +45,7 @@ struct dalm_oracle {
     double err, tol, relax, pc_relax;
     double avg_div, max_cfl;
     int sum_order; /* 0: the reference's serial sums; 1: pairwise (test only) */
+    int limiter;   /* 0: the reference's b=4 limiter, 1: van Albada (extension) */
     /* runtime (src/solver.h:176-205) */
     int64_t step, max_step, tavg_count;
     double tavg_start_time;
@@ -246,14 +247,33 @@ void oracle_destroy(dalm_oracle *o) {
 
 /* ------------------------------------------------------ momentum predictor */
 
-/* κ=1/3 MUSCL face reconstruction with the b=(3-κ)/(1-κ) limiter and upwind
- * flux along one axis, src/cfd.h:37-60 */
+/* The smooth van Albada limiter (an extension: the reference has only the
+ * b=4 limiter): face value f +- (s/4)[(1 - k s) a + (1 + k s) b] with the
+ * switch s = (2ab + eps)/(a^2 + b^2 + eps), eps = 1e-12 (van Albada, van
+ * Leer & Roberts 1982, kappa-MUSCL form); the GPU uses the same operations. */
+static double va_switch(double a, double b) {
+    const double eps = 1e-12;
+    return (2. * a * b + eps) / (a * a + b * b + eps);
+}
+
+/* κ=1/3 MUSCL face reconstruction with the b=(3-κ)/(1-κ) limiter (or van
+ * Albada, limiter 1) and upwind flux along one axis, src/cfd.h:37-60 */
 static void muscl_axis(double fmm, double fm, double fc, double fp, double fpp, double Jp,
-                       double Jm, double *flux_p, double *flux_m) {
+                       double Jm, double *flux_p, double *flux_m, int limiter) {
     const double kap = 1. / 3.;
     const double bb = (3. - kap) / (1. - kap);
     const double e = 1.;
     double d4 = fpp - fp, d3 = fp - fc, d2 = fc - fm, d1 = fm - fmm;
+    if (limiter == 1) {
+        const double sp = va_switch(d4, d3), sc = va_switch(d3, d2), sm = va_switch(d2, d1);
+        const double fpr = fp - (sp / 4.) * ((1. - kap * sp) * d4 + (1. + kap * sp) * d3);
+        const double fpl = fc + (sc / 4.) * ((1. - kap * sc) * d2 + (1. + kap * sc) * d3);
+        const double fmr = fc - (sc / 4.) * ((1. - kap * sc) * d3 + (1. + kap * sc) * d2);
+        const double fml = fm + (sm / 4.) * ((1. - kap * sm) * d1 + (1. + kap * sm) * d2);
+        *flux_p = 0.5 * (Jp * (fpr + fpl) - fabs(Jp) * (fpr - fpl));
+        *flux_m = 0.5 * (Jm * (fmr + fml) - fabs(Jm) * (fmr - fml));
+        return;
+    }
     double s4 = sgn(d4), s3 = sgn(d3), s2 = sgn(d2), s1 = sgn(d1);
     double g6 = s4 * fmax(0., fmin(fabs(d4), s4 * bb * d3));
     double g5 = s3 * fmax(0., fmin(fabs(d3), s3 * bb * d4));
@@ -289,9 +309,12 @@ static void predictor_cell(dalm_oracle *o, int64_t i, int64_t j, int64_t k) {
     for (int m = 0; m < 3; m++) {
         double fc = V[c * 3 + m];
         double fE, fW, fN, fS, fT, fB;
-        muscl_axis(V[ww * 3 + m], V[w * 3 + m], fc, V[e * 3 + m], V[ee * 3 + m], JUE, JUW, &fE, &fW);
-        muscl_axis(V[ss * 3 + m], V[s * 3 + m], fc, V[n * 3 + m], V[nn * 3 + m], JVN, JVS, &fN, &fS);
-        muscl_axis(V[bb * 3 + m], V[b * 3 + m], fc, V[t * 3 + m], V[tt * 3 + m], JWT, JWB, &fT, &fB);
+        muscl_axis(V[ww * 3 + m], V[w * 3 + m], fc, V[e * 3 + m], V[ee * 3 + m], JUE, JUW, &fE, &fW,
+                   o->limiter);
+        muscl_axis(V[ss * 3 + m], V[s * 3 + m], fc, V[n * 3 + m], V[nn * 3 + m], JVN, JVS, &fN, &fS,
+                   o->limiter);
+        muscl_axis(V[bb * 3 + m], V[b * 3 + m], fc, V[t * 3 + m], V[tt * 3 + m], JWT, JWB, &fT, &fB,
+                   o->limiter);
         double conv = (fE - fW + fN - fS + fT - fB) / J;
         double diff = visc * (((V[e * 3 + m] - fc) / (o->x[i + 1] - o->x[i]) -
                                (fc - V[w * 3 + m]) / (o->x[i] - o->x[i - 1])) / dxc +
@@ -1040,6 +1063,7 @@ void oracle_set_poisson(dalm_oracle *o, int64_t max_it, double tol) {
 }
 
 void oracle_set_sum_order(dalm_oracle *o, int mode) { o->sum_order = mode; }
+void oracle_set_limiter(dalm_oracle *o, int limiter) { o->limiter = limiter; }
 
 void oracle_turbines(const dalm_oracle *o, double *torque, double *thrust) {
     for (int64_t w = 0; w < o->wt_count; w++) {

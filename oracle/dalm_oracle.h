@@ -79,6 +79,8 @@ void oracle_set_poisson(dalm_oracle *o, int64_t max_it, double tol);
 /* Test-only: 1 sums dot products pairwise instead of serially (measures the
  * solver's sensitivity to summation order); 0 (default) is the reference. */
 void oracle_set_sum_order(dalm_oracle *o, int mode);
+/* 0: the reference's b=4 limiter (default), 1: the smooth van Albada limiter */
+void oracle_set_limiter(dalm_oracle *o, int limiter);
 void oracle_turbines(const dalm_oracle *o, double *torque, double *thrust);
 void oracle_points(const dalm_oracle *o, double *xyz, double *f, double *torque,
                    double *thrust);

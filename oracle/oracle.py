@@ -328,6 +328,10 @@ class CRestatement(_Base):
         """Test-only: 1 sums dot products pairwise instead of serially."""
         self.lib.oracle_set_sum_order(self.h, int(mode))
 
+    def set_limiter(self, limiter: int):
+        """0: the reference's b=4 limiter; 1: the smooth van Albada limiter."""
+        self.lib.oracle_set_limiter(self.h, int(limiter))
+
     def close(self):
         if self.h:
             self.lib.oracle_destroy(self.h)

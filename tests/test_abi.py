@@ -93,14 +93,13 @@ def test_solver_without_gpu_fails_loudly(make_case):
         pkg.Solver(d)
 
 
-def test_reserved_options_report_unsupported(lib, make_case):
+def test_unknown_options_are_rejected(lib, make_case):
     pkg = package()
     spec, mesh, d, U0, prof = make_case("tiny-bicg")
-    o = pkg.Options()
-    lib.dalm_default_options(C.byref(o))
-    o.limiter = pkg.VAN_ALBADA
-    h = C.c_void_p()
-    assert lib.dalm_create(d.encode(), C.byref(o), C.byref(h)) == 6 and not h.value
-    assert b"van Albada" in lib.dalm_last_error(None)
-    o.limiter = 7
-    assert lib.dalm_create(d.encode(), C.byref(o), C.byref(h)) == 1
+    for field in ("limiter", "precision"):
+        o = pkg.Options()
+        lib.dalm_default_options(C.byref(o))
+        setattr(o, field, 7)
+        h = C.c_void_p()
+        assert lib.dalm_create(d.encode(), C.byref(o), C.byref(h)) == 1 and not h.value
+        assert b"unknown" in lib.dalm_last_error(None)

@@ -214,3 +214,34 @@ def test_kernel_timings(make_case):
     assert kt["jacobi_sweep"]["bytes_per_launch"] > 0
     stages, launches = s.timings()
     assert stages["poisson"] > 0 and launches > 0
+
+
+@pytest.mark.parametrize("name", ["tiny-sor", "tiny-bicg"])
+def test_van_albada_reference_sums_bit_identical(make_case, name):
+    """The smooth limiter (extension) against its restatement in the oracle."""
+    pkg = package()
+    spec, mesh, d, U0, prof = make_case(name)
+    s = pkg.Solver(d, reference_sums=True, limiter=pkg.VAN_ALBADA)
+    o = O.CRestatement(d)
+    o.set_limiter(1)
+    for x in (s, o):
+        x.set_state(U0)
+    for n in range(6):
+        s.step(1)
+        o.step(1)
+        assert s.stats()["it"] == o.stats()["it"], n
+        assert_identical(s, o, ("U", "p"), f"van Albada step {n}")
+
+
+def test_van_albada_fast_mode_with_turbines(make_case):
+    pkg = package()
+    spec, mesh, d, U0, prof = make_case("tiny-turbine")
+    s = pkg.Solver(d, limiter=pkg.VAN_ALBADA)
+    o = O.CRestatement(d)
+    o.set_limiter(1)
+    for x in (s, o):
+        x.set_state(U0)
+    for n in range(6):
+        s.step(1)
+        o.step(1)
+        within_envelope(s, o, n, "van Albada")

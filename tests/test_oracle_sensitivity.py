@@ -81,3 +81,21 @@ def test_summation_order_spread_on_multi_tile_grid(make_case):
     # beyond the tiny cases' envelope, within this grid's
     assert spread["U"] > ENVELOPE["U"]
     assert spread["U"] <= ENVELOPE_MULTI["U"] and spread["p"] <= ENVELOPE_MULTI["p"]
+
+
+def test_van_albada_limiter_in_the_oracle(make_case):
+    """The smooth limiter (an extension) changes the convection, stays
+    close to the reference's limiter on a smooth flow, and runs stably."""
+    spec, mesh, d, U0, prof = make_case("tiny-bicg")
+    out = {}
+    for lim in (0, 1):
+        o = O.CRestatement(d)
+        o.set_limiter(lim)
+        o.set_state(U0)
+        for _ in range(4):
+            o.step(1)
+        out[lim] = o.field("U")
+        assert np.all(np.isfinite(out[lim]))
+        o.close()
+    r = np.linalg.norm(out[1] - out[0]) / np.linalg.norm(out[0])
+    assert 1e-9 < r < 1e-2, r
