@@ -59,6 +59,19 @@ __device__ __forceinline__ void muscl_axis(double fmm, double fm, double fc, dou
 
 __device__ __forceinline__ double sq(double v) { return v * v; }
 
+// Loop over the cells of a Segments box: each block takes (32 k) x (8 j)
+// column segments and marches along i, so the per-cell index arithmetic is
+// done once per segment instead of per cell.  The body sees i, j, k;
+// `continue` skips to the next cell.
+#define TILE_LOOP(S)                                                      \
+    for (int u_ = blockIdx.x; u_ < (S).count; u_ += gridDim.x) {          \
+        int i0_, i1_, j, k;                                               \
+        if (!(S).column(u_, i0_, i1_, j, k)) continue;                    \
+        for (int i = i0_; i < i1_; i++) {
+#define TILE_END \
+        }        \
+    }
+
 // Smagorinsky viscosity at (i,j,k) from the velocity (src/cfd.h:786-825).
 // The filter factor (Cs cbrt(dx dy dz))^2 comes precomputed per cell.
 __device__ __forceinline__ double smagorinsky(const StepParams &P, Vec3<const double> U, int i,
@@ -98,13 +111,11 @@ __device__ __forceinline__ bool interior(const Grid &g, int i, int j, int k) {
 // old one.  nut is the Smagorinsky viscosity of Uold, which is exactly the
 // array the reference computed at the end of the previous step (calc_nut
 // after apply_Ubc, src/solver.h:1157-1164), so it is evaluated inline.
-__global__ void __launch_bounds__(TILE_THREADS)
-k_predict(StepParams P, Tiling T, Vec3<const double> V, Vec3<double> Un, Vec3<const double> JU,
+__global__ void __launch_bounds__(TILE_THREADS, 2)
+k_predict(StepParams P, Segments T, Vec3<const double> V, Vec3<double> Un, Vec3<const double> JU,
           Vec3<const double> F) {
     const Grid &g = P.g;
-    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
-        int i, j, k;
-        if (!T.cell(tile, i, j, k)) continue;
+    TILE_LOOP(T)
         long long c = g.at(i, j, k);
         if (!interior(g, i, j, k)) {
             Un.c[0][c] = V.c[0][c];
@@ -142,7 +153,7 @@ k_predict(StepParams P, Tiling T, Vec3<const double> V, Vec3<double> Un, Vec3<co
             double fm = has_f ? F.c[m][c] : 0.0;
             Un.c[m][c] = fc + P.dt * (-conv + diff + fm);
         }
-    }
+    TILE_END
 }
 
 // ------------------------------------------- face fluxes, their BCs, RHS
@@ -184,11 +195,9 @@ __device__ __forceinline__ double face_z(const StepParams &P, Vec3<const double>
 // west/south/bottom faces, which it recomputes (same arithmetic, same bits).
 template <bool RHS>
 __global__ void __launch_bounds__(TILE_THREADS)
-k_flux_rhs(StepParams P, Tiling T, Vec3<const double> U, Vec3<double> JU, double *b) {
+k_flux_rhs(StepParams P, Segments T, Vec3<const double> U, Vec3<double> JU, double *b) {
     const Grid &g = P.g;
-    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
-        int i, j, k;
-        if (!T.cell(tile, i, j, k)) continue;
+    TILE_LOOP(T)
         long long c = g.at(i, j, k);
         double fe = face_x(P, U, i, j, k), fn = face_y(P, U, i, j, k), ft = face_z(P, U, i, j, k);
         JU.c[0][c] = fe;
@@ -201,7 +210,7 @@ k_flux_rhs(StepParams P, Tiling T, Vec3<const double> U, Vec3<double> JU, double
             double divergence = (fe - fw + fn - fs + ft - fb) / J;
             b[c] = divergence / (P.dt * P.max_diag);
         }
-    }
+    TILE_END
 }
 
 // ------------------------------------------------------------- projection
@@ -288,13 +297,11 @@ __device__ __forceinline__ double proj_face(const StepParams &P, Vec3<double> JU
 // in the same launch, the projected flux goes to a second buffer (JUout) and
 // the host swaps the two.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_project(StepParams P, Tiling T, Vec3<double> U, Vec3<double> JUin, Vec3<double> JUout,
+k_project(StepParams P, Segments T, Vec3<double> U, Vec3<double> JUin, Vec3<double> JUout,
           const double *p, Partials<2> part, DiagState *diag) {
     const Grid &g = P.g;
     double div2 = 0, cfl = 0;
-    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
-        int i, j, k;
-        if (!T.cell(tile, i, j, k)) continue;
+    TILE_LOOP(T)
         long long c = g.at(i, j, k);
         double fe = proj_face(P, JUin, p, 0, i, j, k);
         double fn = proj_face(P, JUin, p, 1, i, j, k);
@@ -321,7 +328,7 @@ k_project(StepParams P, Tiling T, Vec3<double> U, Vec3<double> JUin, Vec3<double
                            fabs(w) * P.dt / P.m.dz[k];
             cfl = local > cfl ? local : cfl;
         }
-    }
+    TILE_END
     if (P.reference_sums) return;  // k_seq_diag sums in the reference's order
     double v[2] = {div2, cfl};
     if (grid_reduce<2>(v, 2u, part) && threadIdx.x == 0) {
@@ -350,17 +357,15 @@ __device__ __forceinline__ double cell_cfl(const StepParams &P, Vec3<const doubl
 
 // Diagnostics alone (after set_state): sum div^2 and max CFL.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_diag(StepParams P, Tiling T, Vec3<const double> U, Vec3<const double> JU, Partials<2> part,
+k_diag(StepParams P, Segments T, Vec3<const double> U, Vec3<const double> JU, Partials<2> part,
        DiagState *diag) {
     double div2 = 0, cfl = 0;
-    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
-        int i, j, k;
-        if (!T.cell(tile, i, j, k)) continue;
+    TILE_LOOP(T)
         double d = cell_div(P, JU, i, j, k);
         div2 += d * d;
         double local = cell_cfl(P, U, i, j, k);
         cfl = local > cfl ? local : cfl;
-    }
+    TILE_END
     double v[2] = {div2, cfl};
     if (grid_reduce<2>(v, 2u, part) && threadIdx.x == 0) {
         diag->div2 = v[0];
@@ -497,35 +502,29 @@ __global__ void k_velocity_bc(StepParams P, Vec3<double> U, Vec3<const double> V
 }
 
 __global__ void __launch_bounds__(TILE_THREADS)
-k_nut_field(StepParams P, Tiling T, Vec3<const double> U, double *nut) {
-    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
-        int i, j, k;
-        if (!T.cell(tile, i, j, k)) continue;
+k_nut_field(StepParams P, Segments T, Vec3<const double> U, double *nut) {
+    TILE_LOOP(T)
         nut[P.g.at(i, j, k)] = smagorinsky(P, U, i, j, k);
-    }
+    TILE_END
 }
 
 __global__ void __launch_bounds__(TILE_THREADS)
-k_div_field(StepParams P, Tiling T, Vec3<const double> JU, double *div) {
+k_div_field(StepParams P, Segments T, Vec3<const double> JU, double *div) {
     const Grid &g = P.g;
-    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
-        int i, j, k;
-        if (!T.cell(tile, i, j, k)) continue;
+    TILE_LOOP(T)
         long long c = g.at(i, j, k);
         double J = P.m.dx[i] * P.m.dy[j] * P.m.dz[k];
         div[c] = (JU.c[0][c] - JU.c[0][g.at(i - 1, j, k)] + JU.c[1][c] -
                   JU.c[1][g.at(i, j - 1, k)] + JU.c[2][c] - JU.c[2][c - 1]) / J;
-    }
+    TILE_END
 }
 
 // Q-criterion on the interior (calc_q_at_cell, src/cfd.h:949-975): central
 // differences over x[i+1] - x[i-1] etc., same operation order.
 __global__ void __launch_bounds__(TILE_THREADS)
-k_q_field(StepParams P, Tiling T, Vec3<const double> U, double *q) {
+k_q_field(StepParams P, Segments T, Vec3<const double> U, double *q) {
     const Grid &g = P.g;
-    for (long long tile = blockIdx.x; tile < T.ntiles; tile += gridDim.x) {
-        int i, j, k;
-        if (!T.cell(tile, i, j, k)) continue;
+    TILE_LOOP(T)
         const long long c = g.at(i, j, k);
         const long long ce = g.at(i + 1, j, k), cw = g.at(i - 1, j, k);
         const long long cn = g.at(i, j + 1, k), cs = g.at(i, j - 1, k);
@@ -544,7 +543,7 @@ k_q_field(StepParams P, Tiling T, Vec3<const double> U, double *q) {
         const double dwdz = (U.c[2][ct] - U.c[2][cb]) / dztb;
         q[c] = -0.5 * (dudx * dudx + dvdy * dvdy + dwdz * dwdz +
                        2 * (dudy * dvdx + dudz * dwdx + dvdz * dwdy));
-    }
+    TILE_END
 }
 
 // Running time average over every stored cell (calc_ax_plus_by,
@@ -623,7 +622,7 @@ int plane_blocks(const Grid &g) {
 
 void launch_predict(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,
                     Vec3<double> unew, Vec3<const double> ju, Vec3<const double> f) {
-    Tiling T = Tiling::make(full_box(P.g));
+    Segments T = Segments::make(full_box(P.g), L.blocks);
     L.pre(KK_PREDICT);
     k_predict<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, uold, unew, ju, f);
     L.post(KK_PREDICT);
@@ -631,7 +630,7 @@ void launch_predict(const LaunchCtx &L, const StepParams &P, Vec3<const double> 
 
 void launch_flux_rhs(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                      Vec3<double> ju, double *b) {
-    Tiling T = Tiling::make(face_box(P.g));
+    Segments T = Segments::make(face_box(P.g), L.blocks);
     L.pre(KK_FLUX_RHS);
     k_flux_rhs<true><<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju, b);
     L.post(KK_FLUX_RHS);
@@ -639,7 +638,7 @@ void launch_flux_rhs(const LaunchCtx &L, const StepParams &P, Vec3<const double>
 
 void launch_flux_only(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                       Vec3<double> ju) {
-    Tiling T = Tiling::make(face_box(P.g));
+    Segments T = Segments::make(face_box(P.g), L.blocks);
     L.pre(KK_FLUX_RHS);
     k_flux_rhs<false><<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju, nullptr);
     L.post(KK_FLUX_RHS);
@@ -654,7 +653,7 @@ void launch_pressure_bc(const LaunchCtx &L, const StepParams &P, double *p) {
 void launch_project(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
                     Vec3<double> ju_in, Vec3<double> ju_out, const double *p, Partials<2> part,
                     DiagState *diag) {
-    Tiling T = Tiling::make(face_box(P.g));
+    Segments T = Segments::make(face_box(P.g), L.blocks);
     L.pre(KK_PROJECT);
     k_project<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju_in, ju_out, p, part, diag);
     L.post(KK_PROJECT);
@@ -675,7 +674,7 @@ void launch_velocity_bc(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
 
 void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                  Vec3<const double> ju, Partials<2> part, DiagState *diag) {
-    Tiling T = Tiling::make(interior_box(P.g));
+    Segments T = Segments::make(interior_box(P.g), L.blocks);
     L.pre(KK_DIAG);
     if (P.reference_sums)
         k_seq_diag<<<1, 32, 0, L.s>>>(P, u, ju, diag);
@@ -685,21 +684,21 @@ void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
 }
 
 void launch_nut_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> u, double *nut) {
-    Tiling T = Tiling::make(interior_box(P.g));
+    Segments T = Segments::make(interior_box(P.g), L.blocks);
     L.pre(KK_LAYOUT);
     k_nut_field<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, nut);
     L.post(KK_LAYOUT);
 }
 
 void launch_div_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> ju, double *div) {
-    Tiling T = Tiling::make(interior_box(P.g));
+    Segments T = Segments::make(interior_box(P.g), L.blocks);
     L.pre(KK_LAYOUT);
     k_div_field<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, ju, div);
     L.post(KK_LAYOUT);
 }
 
 void launch_q_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> u, double *q) {
-    Tiling T = Tiling::make(interior_box(P.g));
+    Segments T = Segments::make(interior_box(P.g), L.blocks);
     L.pre(KK_LAYOUT);
     k_q_field<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, q);
     L.post(KK_LAYOUT);
