@@ -100,6 +100,23 @@ def parse():
     return ap.parse_args()
 
 
+def mixed_errors(a, b):
+    """Relative L2 error of the mixed form's final state against the FP64
+    form's after the same steps: per velocity component, pressure, and per
+    turbine thrust / power."""
+    import numpy as np
+
+    def rel(x, y):
+        ny = np.linalg.norm(y)
+        return float(np.linalg.norm(x - y) / (ny if ny > 0 else 1.0))
+    out = {f"U[{m}]": rel(a["U"][..., m], b["U"][..., m]) for m in range(3)}
+    out["p"] = rel(a["p"], b["p"])
+    (tha, _, pwa), (thb, _, pwb) = a["turbines"], b["turbines"]
+    out["thrust"] = [float(abs(x - y) / abs(y)) if y else 0.0 for x, y in zip(tha, thb)]
+    out["power"] = [float(abs(x - y) / abs(y)) if y else 0.0 for x, y in zip(pwa, pwb)]
+    return out
+
+
 def max_over_ranks(v, world):
     """The largest of every rank's v (the job's time is its slowest replica's)."""
     if world == 1:
@@ -343,21 +360,23 @@ def run_ours(args):
         ms = e0.elapsed_time(e1)
         _, launches = s.timings()
         ms = max_over_ranks(ms, world)
+        final = {"U": s.field("U"), "p": s.field("p"), "turbines": s.turbines()}
         s.finalize()
-        return ms, its, errs, clk, launches
+        return ms, its, errs, clk, launches, final
 
     # ---- the reference's precision: the headline
-    ms, its, errs, clk, launches = timed_region(pkg.FP64)
+    ms, its, errs, clk, launches, final64 = timed_region(pkg.FP64)
     value = whole_job_rate(n_int, args.steps, world, ms / 1e3)
     # ---- the mixed-precision form on the same steps
     mixed = None
     if not args.no_mixed:
-        mms, mits, merrs, mclk, _ = timed_region(pkg.MIXED)
+        mms, mits, merrs, mclk, _, finalm = timed_region(pkg.MIXED)
         mvalue = whole_job_rate(n_int, args.steps, world, mms / 1e3)
         mixed = {"value": mvalue, "unit": METRIC, "ms_per_step": mms / args.steps,
                  "vs_fp64": mvalue / value, "poisson_iterations": mits,
                  "max_residual": max(merrs), "fp64_max_residual": max(errs),
                  "tolerance": spec.tol, "clocks": mclk,
+                 "error_vs_fp64": mixed_errors(finalm, final64),
                  "how": "DALM_MIXED: FP64 iterative refinement with capped FP32 BiCGStab passes, "
                         "FP64 fallback when a pass stalls; stop test on the FP64 residual"}
 
