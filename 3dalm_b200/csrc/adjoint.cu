@@ -1,0 +1,155 @@
+// Discrete-adjoint kernels (FP64).  Each kernel applies one transposed
+// stage of the time step (adjoint_cell.cuh) as a gather: every output
+// element is written by one thread, so the results do not depend on
+// scheduling and need no atomics; the one sum over cells (the adjoint
+// pressure right-hand side's norm) uses the deterministic grid reduction.
+#include "adjoint.cuh"
+
+namespace dalm {
+
+namespace {
+
+// grid-stride loop over the cells of a box, k fastest (coalesced rows)
+template <typename F>
+__device__ __forceinline__ void box_loop(const Box &b, F f) {
+    const long long nk = b.hi[2] - b.lo[2], nj = b.hi[1] - b.lo[1], ni = b.hi[0] - b.lo[0];
+    const long long tot = ni * nj * nk;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < tot;
+         n += (long long)gridDim.x * blockDim.x) {
+        int k = b.lo[2] + (int)(n % nk);
+        long long r = n / nk;
+        int j = b.lo[1] + (int)(r % nj);
+        int i = b.lo[0] + (int)(r / nj);
+        f(i, j, k);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_adj_velocity_bc(adj::AdjBcArgs A, long long n0, long long n1) {
+    for (long long n = n0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; n < n1;
+         n += (long long)gridDim.x * blockDim.x)
+        adj::adj_velocity_bc_column(A, n);
+}
+
+__global__ void __launch_bounds__(256)
+k_adj_project(adj::AdjProjectArgs A, Box box, Partials<1> part, double *sumsq) {
+    double acc = 0;
+    box_loop(box, [&](int i, int j, int k) { acc += adj::adj_project_cell(A, i, j, k); });
+    double v[1] = {acc};
+    if (grid_reduce<1>(v, 0u, part) && threadIdx.x == 0) *sumsq = v[0];
+}
+
+__global__ void __launch_bounds__(256) k_adj_faces(adj::AdjFacesArgs A, Box box) {
+    box_loop(box, [&](int i, int j, int k) { adj::adj_faces_cell(A, i, j, k); });
+}
+
+__global__ void __launch_bounds__(256) k_adj_nut(adj::AdjNutArgs A, Box box) {
+    box_loop(box, [&](int i, int j, int k) { adj::adj_nut_cell(A, i, j, k); });
+}
+
+__global__ void __launch_bounds__(256) k_adj_predict(adj::AdjPredictArgs A, Box box) {
+    box_loop(box, [&](int i, int j, int k) { adj::adj_predict_cell(A, i, j, k); });
+}
+
+// one block per blade point: the six sums over its support, reduced in a
+// fixed order
+__global__ void __launch_bounds__(256)
+k_adj_alm_gather(StepParams P, AlmDev A, Vec3<const double> af, double *out) {
+    __shared__ double smem[32 * 6];
+    const int a = blockIdx.x;
+    int lo[3], hi[3];
+    adj::alm_support_box(P, A, a, lo, hi);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    Box b{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}};
+    if (!b.empty()) {
+        const long long nk = b.hi[2] - b.lo[2], nj = b.hi[1] - b.lo[1], ni = b.hi[0] - b.lo[0];
+        const long long tot = ni * nj * nk;
+        for (long long n = threadIdx.x; n < tot; n += blockDim.x) {
+            int k = b.lo[2] + (int)(n % nk);
+            long long r = n / nk;
+            int j = b.lo[1] + (int)(r % nj);
+            int i = b.lo[0] + (int)(r / nj);
+            adj::adj_alm_gather_term(P, A, af, a, i, j, k, acc);
+        }
+    }
+    block_reduce<6>(acc, 0u, smem);
+    if (threadIdx.x == 0)
+        for (int m = 0; m < 6; m++) out[6 * (long long)a + m] = acc[m];
+}
+
+__global__ void k_adj_alm_point(adj::AdjAlmPointArgs X) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < X.A.ap_count) adj::adj_alm_point(X, a);
+}
+
+__global__ void k_adj_alm_scatter(adj::AdjAlmPointArgs X, Vec3<double> aU, double *grad) {
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        adj::adj_alm_scatter(X.A, X.ids, X.w, X.lU, X.gth, X.torque, X.weight, aU, grad);
+}
+
+int grid_for(long long n, int cap) {
+    long long b = (n + 255) / 256;
+    if (b < 1) b = 1;
+    return (int)(b < cap ? b : cap);
+}
+
+}  // namespace
+
+void launch_adj_velocity_bc(const LaunchCtx &L, const adj::AdjBcArgs &A) {
+    const Grid &g = A.P.g;
+    long long nyz = (long long)g.nj() * g.nk(), nxz = (long long)g.ni() * g.nk(),
+              nxy = (long long)g.ni() * g.nj();
+    long long mid = 2 * (nyz + nxz), tot = mid + 2 * nxy;
+    L.pre(KK_ADJ_BC);
+    k_adj_velocity_bc<<<grid_for(mid, L.blocks), 256, 0, L.s>>>(A, 0, mid);
+    L.post(KK_ADJ_BC);
+    L.pre(KK_ADJ_BC);
+    k_adj_velocity_bc<<<grid_for(tot - mid, L.blocks), 256, 0, L.s>>>(A, mid, tot);
+    L.post(KK_ADJ_BC);
+}
+
+void launch_adj_project(const LaunchCtx &L, const adj::AdjProjectArgs &A, Partials<1> part,
+                        double *sumsq) {
+    const Grid &g = A.P.g;
+    Box box{{g.gc, g.gc, g.gc}, {g.nx - g.gc, g.ny - g.gc, g.nz - g.gc}};
+    L.pre(KK_ADJ_PROJECT);
+    k_adj_project<<<L.blocks, 256, 0, L.s>>>(A, box, part, sumsq);
+    L.post(KK_ADJ_PROJECT);
+}
+
+void launch_adj_faces(const LaunchCtx &L, const adj::AdjFacesArgs &A) {
+    const Grid &g = A.P.g;
+    // the interior and the first outflow guide plane (the outlet face reads it)
+    Box box{{g.gc, g.gc, g.gc}, {g.nx - g.gc + 1, g.ny - g.gc, g.nz - g.gc}};
+    L.pre(KK_ADJ_FACES);
+    k_adj_faces<<<L.blocks, 256, 0, L.s>>>(A, box);
+    L.post(KK_ADJ_FACES);
+}
+
+void launch_adj_predict(const LaunchCtx &L, const adj::AdjNutArgs &N, const adj::AdjPredictArgs &A) {
+    const Grid &g = A.P.g;
+    Box inner{{g.gc, g.gc, g.gc}, {g.nx - g.gc, g.ny - g.gc, g.nz - g.gc}};
+    Box all{{0, 0, 0}, {g.nx, g.ny, g.nz}};
+    L.pre(KK_ADJ_NUT);
+    k_adj_nut<<<L.blocks, 256, 0, L.s>>>(N, inner);
+    L.post(KK_ADJ_NUT);
+    L.pre(KK_ADJ_PREDICT);
+    k_adj_predict<<<L.blocks, 256, 0, L.s>>>(A, all);
+    L.post(KK_ADJ_PREDICT);
+}
+
+void launch_adj_alm(const LaunchCtx &L, const StepParams &P, const AlmDev &A,
+                    Vec3<const double> af, const adj::AdjAlmPointArgs &X, Vec3<double> aU,
+                    double *grad) {
+    if (A.ap_count <= 0) return;
+    L.pre(KK_ADJ_ALM);
+    k_adj_alm_gather<<<A.ap_count, 256, 0, L.s>>>(P, A, af, const_cast<double *>(X.gather));
+    L.post(KK_ADJ_ALM);
+    L.pre(KK_ADJ_ALM);
+    k_adj_alm_point<<<(A.ap_count + 63) / 64, 64, 0, L.s>>>(X);
+    L.post(KK_ADJ_ALM);
+    L.pre(KK_ADJ_ALM);
+    k_adj_alm_scatter<<<1, 32, 0, L.s>>>(X, aU, grad);
+    L.post(KK_ADJ_ALM);
+}
+
+}  // namespace dalm

@@ -256,6 +256,8 @@ enum KernelKind {
     KK_POISSON_BEGIN, KK_LAYOUT, KK_SEQ_SUM, KK_BICG_PF, KK_BICG_SF, KK_REFINE_RESIDUAL, KK_REFINE_UPDATE,
     // FP32 inner solves of iterative refinement
     KK_SOR_SWEEP32, KK_JACOBI_SWEEP32, KK_BICG_P32, KK_BICG_Q32, KK_BICG_S32, KK_BICG_T32, KK_BICG_XR32,
+    // discrete adjoint
+    KK_ADJ_BC, KK_ADJ_PROJECT, KK_ADJ_FACES, KK_ADJ_NUT, KK_ADJ_PREDICT, KK_ADJ_ALM,
     KK_COUNT
 };
 

@@ -50,7 +50,8 @@ const char *kKindNames[KK_COUNT] = {
     "bicg_init", "bicg_p", "bicg_q", "bicg_s", "bicg_t", "bicg_xr",
     "poisson_begin", "layout", "seq_sum", "bicg_p_fused", "bicg_s_fused", "refine_residual",
     "refine_update", "sor_sweep32", "jacobi_sweep32", "bicg_p32", "bicg_q32", "bicg_s32",
-    "bicg_t32", "bicg_xr32"};
+    "bicg_t32", "bicg_xr32", "adj_velocity_bc", "adj_project", "adj_faces", "adj_nut",
+    "adj_predict", "adj_alm"};
 
 }  // namespace
 
