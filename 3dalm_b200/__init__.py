@@ -39,7 +39,8 @@ EXPORTS = (
     "dalm_step", "dalm_run_stage", "dalm_advance_clock", "dalm_get_step_stats",
     "dalm_set_poisson", "dalm_get_counts", "dalm_get_turbines", "dalm_get_points",
     "dalm_synchronize", "dalm_get_stream", "dalm_get_timings", "dalm_kernel_kinds",
-    "dalm_get_kernel_timing", "dalm_diagnostics_noalloc",
+    "dalm_get_kernel_timing", "dalm_diagnostics_noalloc", "dalm_get_turbine_params",
+    "dalm_adjoint_power_grad", "dalm_get_adjoint_stats",
 )
 
 
@@ -212,6 +213,33 @@ class Solver:
         cv = [None if v is None else np.ascontiguousarray(v, dtype=np.float64)
               for v in (yaw, pitch, omega)]
         self._check(self.lib.dalm_set_turbine_params(self.h, *[_p(v) for v in cv]))
+
+    def turbine_params(self):
+        """(yaw_deg, pitch_deg, omega) per turbine."""
+        n = self.turbine_count
+        yaw, pitch, om = np.zeros(n), np.zeros(n), np.zeros(n)
+        if n:
+            self._check(self.lib.dalm_get_turbine_params(self.h, _p(yaw), _p(pitch), _p(om)))
+        return yaw, pitch, om
+
+    def power_gradient(self, t0: int, t1: int, ckpt_every: int = 20):
+        """Discrete adjoint (dalm_adjoint_power_grad): runs the steps through
+        t1 and returns (J, grad) with J the mean total power over steps
+        t0..t1 and grad[w] = dJ/d(yaw_deg, pitch_deg, omega) of turbine w."""
+        n = self.turbine_count
+        grad = np.zeros(3 * max(n, 1))
+        J = C.c_double()
+        self._check(self.lib.dalm_adjoint_power_grad(self.h, int(t0), int(t1), int(ckpt_every),
+                                                      _p(grad), C.byref(J)))
+        return float(J.value), grad[:3 * n].reshape(n, 3)
+
+    def adjoint_stats(self) -> dict:
+        solves, its, rec = C.c_int64(), C.c_int64(), C.c_int64()
+        res = C.c_double()
+        self._check(self.lib.dalm_get_adjoint_stats(self.h, C.byref(solves), C.byref(its),
+                                                     C.byref(res), C.byref(rec)))
+        return {"solves": solves.value, "iterations": its.value,
+                "max_rel_residual": res.value, "recomputed_steps": rec.value}
 
     def set_poisson(self, max_it: int, tol: float):
         self._check(self.lib.dalm_set_poisson(self.h, C.c_int64(max_it), C.c_double(tol)))

@@ -86,6 +86,12 @@ __global__ void k_adj_alm_scatter(adj::AdjAlmPointArgs X, Vec3<double> aU, doubl
         adj::adj_alm_scatter(X.A, X.ids, X.w, X.lU, X.gth, X.torque, X.weight, aU, grad);
 }
 
+__global__ void k_adj_scale(double *v, long long n, double s) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        v[i] *= s;
+}
+
 int grid_for(long long n, int cap) {
     long long b = (n + 255) / 256;
     if (b < 1) b = 1;
@@ -135,6 +141,12 @@ void launch_adj_predict(const LaunchCtx &L, const adj::AdjNutArgs &N, const adj:
     L.pre(KK_ADJ_PREDICT);
     k_adj_predict<<<L.blocks, 256, 0, L.s>>>(A, all);
     L.post(KK_ADJ_PREDICT);
+}
+
+void launch_adj_scale(const LaunchCtx &L, double *v, long long n, double s) {
+    L.pre(KK_ADJ_PROJECT);
+    k_adj_scale<<<grid_for(n, L.blocks), 256, 0, L.s>>>(v, n, s);
+    L.post(KK_ADJ_PROJECT);
 }
 
 void launch_adj_alm(const LaunchCtx &L, const StepParams &P, const AlmDev &A,

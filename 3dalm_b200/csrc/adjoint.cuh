@@ -11,6 +11,8 @@ void launch_adj_velocity_bc(const LaunchCtx &L, const adj::AdjBcArgs &A);
 // adjoint pressure right-hand side on the interior; writes sum(rhs^2) to *sumsq
 void launch_adj_project(const LaunchCtx &L, const adj::AdjProjectArgs &A, Partials<1> part,
                         double *sumsq);
+// v[0..n) *= s
+void launch_adj_scale(const LaunchCtx &L, double *v, long long n, double s);
 // transposed face interpolation + Poisson right-hand side, into A.aus
 void launch_adj_faces(const LaunchCtx &L, const adj::AdjFacesArgs &A);
 // transposed predictor: viscosity pass, then the stencil gather

@@ -5,6 +5,7 @@
 // (src/solver.h:1034-1306); the only host synchronisation inside a step is
 // the Poisson loop's convergence poll, once per batch of iterations.
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -17,6 +18,7 @@
 #include <vector>
 
 #include "../../include/dalm.h"
+#include "adjoint.cuh"
 #include "alm.cuh"
 #include "case_io.hpp"
 #include "output_io.hpp"
@@ -42,6 +44,9 @@ constexpr double INNER_RTOL = 1e-3;
 constexpr long long INNER_CAP = 100;
 constexpr double STALL = 0.85;
 constexpr long long MAX_REFINE = 1000;
+// Adjoint pressure solves stop at this RMS residual relative to the RMS of
+// their right-hand side.
+constexpr double ADJ_RTOL = 1e-10;
 
 const char *kKindNames[KK_COUNT] = {
     "predict", "flux_rhs", "pressure_bc", "project", "velocity_bc", "diag", "tavg",
@@ -122,6 +127,8 @@ struct dalm_handle {
     std::vector<double> base_twist, twist;
     double *h_wt_out = nullptr;  // pinned: torque[T], thrust[T]
     Box fbox{{0, 0, 0}, {0, 0, 0}};
+    std::vector<double> pitch_deg;  // collective pitch per turbine (dalm_set_turbine_params)
+    double last_alm_time = 0;       // time of the last actuator-line evaluation
     // runtime
     int64_t step = 0, tavg_count = 0, last_it = 0;
     int64_t max_it = 0;
@@ -434,6 +441,7 @@ struct dalm_handle {
         }
         base_twist = cs.ap_twist;
         twist = cs.ap_twist;
+        pitch_deg.assign((size_t)T, 0.0);
         alm.wt = upload(h_wt);
         alm.r = upload(cs.ap_r);
         alm.dr = upload(cs.ap_dr);
@@ -702,10 +710,11 @@ struct dalm_handle {
         return u;
     }
 
-    void stage_alm() {
+    void stage_alm() { alm_at(cs.dt * (double)step); }  // rt.get_time(), src/solver.h:189-191
+    void alm_at(double tm) {
         if (alm.ap_count == 0) return;
         StageTimer t(this, DALM_STAGE_ALM);
-        double tm = cs.dt * (double)step;  // rt.get_time(), src/solver.h:189-191
+        last_alm_time = tm;
         launch_alm_points(L, P, alm, tm, c(u_cur()));
         Box cur = force_box(tm);
         launch_alm_project(L, P, alm, unite(fbox, cur), f3());
@@ -903,6 +912,294 @@ struct dalm_handle {
         }
     }
 
+    // ---- discrete adjoint of the time stepping ------------------------------
+    //
+    // J = mean over steps t0..t1 of the total turbine power; its gradient with
+    // respect to every turbine's yaw (deg), collective pitch (deg) and rotor
+    // speed (rad/s).  The forward run from the current state stores a
+    // restart point every k steps; the reverse sweep takes the segments last
+    // to first, recomputes each from its restart point while recording the
+    // velocity and face fluxes of every step, then runs the transposed steps
+    // (adjoint_cell.cuh) backwards through it.  The adjoint pressure solve
+    // reuses the forward solver: A^T = M A M^-1 with M the cell volumes.
+    struct AdjointStats {
+        long long solves = 0, iterations = 0, recomputed_steps = 0;
+        double max_rel_residual = 0;
+    } adj_stats;
+    long long adj_hint = 0;
+
+    // device buffers of one gradient run, freed when it ends
+    struct Scratch {
+        std::vector<void *> ptrs;
+        ~Scratch() {
+            for (void *p : ptrs) cudaFree(p);
+        }
+        template <typename T>
+        T *get(size_t n) {
+            void *p = nullptr;
+            DALM_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+            ptrs.push_back(p);
+            return (T *)p;
+        }
+    };
+    // a restart point: the fields a step reads and the host-side step state
+    struct Snapshot {
+        double *U[3], *JU[3], *F[3], *p;
+        int64_t step, last_it;
+        Box fbox;
+        double alm_time;
+    };
+    void alloc_snapshot(Scratch &S, Snapshot &c) {
+        for (int m = 0; m < 3; m++) {
+            c.U[m] = S.get<double>(g.total);
+            c.JU[m] = S.get<double>(g.total);
+            c.F[m] = S.get<double>(g.total);
+        }
+        c.p = S.get<double>(g.total);
+    }
+    void d2d(double *dst, const double *src, size_t n = 0) {
+        DALM_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * (n ? n : (size_t)g.total),
+                                  cudaMemcpyDeviceToDevice, stream));
+    }
+    void zero(double *p, size_t n = 0) {
+        DALM_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * (n ? n : (size_t)g.total), stream));
+    }
+    void save(Snapshot &c) {
+        for (int m = 0; m < 3; m++) {
+            d2d(c.U[m], U[ucur][m]);
+            d2d(c.JU[m], JU[jcur][m]);
+            d2d(c.F[m], F[m]);
+        }
+        d2d(c.p, Pp);
+        c.step = step;
+        c.last_it = last_it;
+        c.fbox = fbox;
+        c.alm_time = last_alm_time;
+    }
+    void load(const Snapshot &c) {
+        for (int m = 0; m < 3; m++) {
+            d2d(U[ucur][m], c.U[m]);
+            d2d(JU[jcur][m], c.JU[m]);
+            d2d(F[m], c.F[m]);
+        }
+        d2d(Pp, c.p);
+        step = c.step;
+        last_it = c.last_it;
+        fbox = c.fbox;
+        last_alm_time = c.alm_time;
+    }
+    // one time step without time averaging or output (recomputation)
+    void integrate_step() {
+        stage_predict();
+        stage_flux_rhs();
+        stage_poisson();
+        stage_project();
+        stage_alm();
+        step++;
+    }
+    // A y = rhs (in B) from the guess in Pp, to an absolute RMS residual
+    long long adjoint_solve(double tol_abs) {
+        double ncell = (double)g.ni() * g.nj() * g.nk();
+        launch_poisson_begin(L, d_kst, max_it, tol_abs, ncell);
+        if (pcfg.method == PM_BICG)
+            launch_bicg_init(L, g, coef, pb, pcfg, Partials<1>{partial, ticket}, d_kst);
+        long long n = run_batches(0, adj_hint > 0 ? adj_hint : last_it, max_it);
+        adj_hint = n;
+        return n;
+    }
+
+    struct AdjBuffers {
+        double *aU[3], *aV[3], *aJU[3], *af[3], *nu, *s6[6], *y, *grad, *sumsq;
+        double *gather, *w, *lU, *gth, *torque;
+        long long *ids;
+    };
+
+    // the transposed actuator line at time t on velocity u (the adjoint of the
+    // force it projected is B.af), with the objective weight of its power
+    void adjoint_alm(AdjBuffers &A, double t, Vec3<const double> u, double weight) {
+        launch_alm_points(L, P, alm, t, u);
+        adj::AdjAlmPointArgs X{P, alm, u, t, weight, A.gather, A.ids, A.w, A.lU, A.gth, A.torque};
+        launch_adj_alm(L, P, alm, Vec3<const double>{{A.af[0], A.af[1], A.af[2]}}, X,
+                       Vec3<double>{{A.aU[0], A.aU[1], A.aU[2]}}, A.grad);
+    }
+
+    // one transposed time step n: V = U^n, JUn = JU^n, U1 = U^{n+1}; on entry
+    // A.aU, A.aJU, A.af hold the adjoints of U^{n+1}, JU^{n+1}, f^{n+1}, on
+    // exit those of U^n, JU^n, f^n
+    void adjoint_step(AdjBuffers &A, int64_t n, double *const *V, double *const *JUn,
+                      double *const *U1, double weight) {
+        const Vec3<const double> v{{V[0], V[1], V[2]}}, ju{{JUn[0], JUn[1], JUn[2]}},
+            u1{{U1[0], U1[1], U1[2]}};
+        Vec3<double> aU{{A.aU[0], A.aU[1], A.aU[2]}}, aV{{A.aV[0], A.aV[1], A.aV[2]}},
+            aJU{{A.aJU[0], A.aJU[1], A.aJU[2]}}, af{{A.af[0], A.af[1], A.af[2]}};
+        adjoint_alm(A, cs.dt * (double)n, u1, weight);
+        launch_adj_velocity_bc(L, adj::AdjBcArgs{P, v, aU, aV});
+        launch_adj_project(L, adj::AdjProjectArgs{P, c(aU), c(aJU), B}, Partials<1>{partial, ticket},
+                           A.sumsq);
+        double sumsq = 0;
+        DALM_CUDA(cudaMemcpyAsync(&sumsq, A.sumsq, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        if (!std::isfinite(sumsq)) throw std::runtime_error("non-finite adjoint pressure right-hand side");
+        if (sumsq > 0) {
+            const double ncell = (double)g.ni() * g.nj() * g.nk();
+            const double rms = std::sqrt(sumsq / ncell);
+            // solved at unit RMS right-hand side (the breakdown test of the
+            // Krylov solver is absolute); the previous step's solution,
+            // scaled alike, is the guess
+            d2d(Pp, A.y);
+            launch_adj_scale(L, Pp, g.total, 1.0 / rms);
+            launch_adj_scale(L, B, g.total, 1.0 / rms);
+            long long it = adjoint_solve(ADJ_RTOL);
+            d2d(A.y, Pp);
+            launch_adj_scale(L, A.y, g.total, rms);
+            adj_stats.solves++;
+            adj_stats.iterations += it;
+            adj_stats.max_rel_residual = std::max(adj_stats.max_rel_residual, h_kst[0].err);
+        } else {
+            zero(A.y);
+        }
+        launch_adj_faces(L, adj::AdjFacesArgs{P, c(aJU), A.y, aU});
+        adj::AdjNutArgs N{P, v, c(aU), A.nu, {}};
+        adj::AdjPredictArgs Q{P, v, ju, c(aU), A.nu, {}, aV, aJU, af};
+        for (int m = 0; m < 6; m++) {
+            N.s6[m] = A.s6[m];
+            Q.s6[m] = A.s6[m];
+        }
+        launch_adj_predict(L, N, Q);
+        for (int m = 0; m < 3; m++) {
+            std::swap(A.aU[m], A.aV[m]);
+            zero(A.aV[m]);
+        }
+    }
+
+    void power_gradient(int64_t t0, int64_t t1, int64_t k, double *grad_out, double *J_out) {
+        const int T = alm.wt_count;
+        if (T == 0) throw Unsupported("the case has no turbines");
+        if (k < 1) throw std::invalid_argument("ckpt_every must be at least 1");
+        const int64_t n_first = std::max<int64_t>(step, 1);
+        if (t0 < n_first || t1 < t0)
+            throw std::invalid_argument("need max(current step, 1) <= t0 <= t1");
+        for (const TurbineDev &w : h_wt)
+            if (w.type != EULER_YAW)
+                throw Unsupported("the gradient needs yaw-type turbine angles "
+                                  "(dalm_set_turbine_params sets them)");
+        adj_stats = AdjointStats{};
+        // the forces the first step reads, from the current velocity and
+        // parameters at the time of the last actuator-line evaluation
+        const double t_init = last_alm_time;
+        alm_at(t_init);
+
+        Scratch S;
+        const int64_t nsteps = t1 - n_first + 1, nseg = (nsteps + k - 1) / k;
+        const int64_t last0 = n_first + (nseg - 1) * k;  // first step of the last segment
+        std::vector<Snapshot> ck((size_t)nseg);
+        for (auto &c : ck) alloc_snapshot(S, c);
+        Snapshot fin;
+        alloc_snapshot(S, fin);
+        double *fin_uold[3];
+        for (int m = 0; m < 3; m++) fin_uold[m] = S.get<double>(g.total);
+        // tape of one segment: U^n for k+1 steps, JU^n for k
+        std::vector<std::array<double *, 3>> tU((size_t)k + 1), tJU((size_t)k);
+        for (auto &a : tU)
+            for (int m = 0; m < 3; m++) a[m] = S.get<double>(g.total);
+        for (auto &a : tJU)
+            for (int m = 0; m < 3; m++) a[m] = S.get<double>(g.total);
+        auto record = [&](int64_t slot, bool with_flux) {
+            for (int m = 0; m < 3; m++) {
+                d2d(tU[(size_t)slot][m], U[ucur][m]);
+                if (with_flux) d2d(tJU[(size_t)slot][m], JU[jcur][m]);
+            }
+        };
+
+        // forward run
+        double J = 0;
+        if (step == 0) step_once();  // step 0: no integration (time average, output)
+        for (int64_t n = n_first; n <= t1; n++) {
+            if ((n - n_first) % k == 0) save(ck[(size_t)((n - n_first) / k)]);
+            if (n >= last0) record(n - last0, true);
+            step_once();
+            if (n >= t0) {
+                DALM_CUDA(cudaStreamSynchronize(stream));
+                for (int w = 0; w < T; w++) J += h_wt_out[w] * std::fabs(h_wt[w].rot_speed);
+            }
+        }
+        record(t1 - last0 + 1, false);
+        J /= (double)(t1 - t0 + 1);
+        if (!std::isfinite(J)) throw std::runtime_error("non-finite power in the forward run");
+        save(fin);
+        for (int m = 0; m < 3; m++) d2d(fin_uold[m], U[1 - ucur][m]);
+        DiagState *fin_diag = S.get<DiagState>(1);
+        KrylovState *fin_kst = S.get<KrylovState>(2);
+        DALM_CUDA(cudaMemcpyAsync(fin_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToDevice, stream));
+        DALM_CUDA(cudaMemcpyAsync(fin_kst, d_kst, 2 * sizeof(KrylovState), cudaMemcpyDeviceToDevice, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        KrylovState fin_hkst[2] = {h_kst[0], h_kst[1]};
+        DiagState fin_hdiag = *h_diag;
+        std::vector<double> fin_wt(h_wt_out, h_wt_out + 2 * T);
+        const int64_t fin_last_it = last_it;
+
+        // reverse sweep
+        AdjBuffers A{};
+        for (int m = 0; m < 3; m++) {
+            A.aU[m] = S.get<double>(g.total);
+            A.aV[m] = S.get<double>(g.total);
+            A.aJU[m] = S.get<double>(g.total);
+            A.af[m] = S.get<double>(g.total);
+            zero(A.aU[m]); zero(A.aV[m]); zero(A.aJU[m]); zero(A.af[m]);
+        }
+        A.nu = S.get<double>(g.total);
+        for (int m = 0; m < 6; m++) A.s6[m] = S.get<double>(g.total);
+        A.y = S.get<double>(g.total);
+        zero(A.y);
+        A.grad = S.get<double>(3 * (size_t)T);
+        zero(A.grad, 3 * (size_t)T);
+        A.sumsq = S.get<double>(1);
+        const size_t ap = (size_t)alm.ap_count;
+        A.gather = S.get<double>(6 * ap);
+        A.ids = S.get<long long>(8 * ap);
+        A.w = S.get<double>(8 * ap);
+        A.lU = S.get<double>(3 * ap);
+        A.gth = S.get<double>(3 * ap);
+        A.torque = S.get<double>(ap);
+        const double weight = 1.0 / (double)(t1 - t0 + 1);
+        for (int64_t s = nseg - 1; s >= 0; s--) {
+            const int64_t n0 = n_first + s * k, n1 = std::min(n0 + k - 1, t1);
+            if (s != nseg - 1) {  // the last segment was recorded by the forward run
+                load(ck[(size_t)s]);
+                for (int64_t n = n0; n <= n1; n++) {
+                    record(n - n0, true);
+                    integrate_step();
+                    adj_stats.recomputed_steps++;
+                }
+                record(n1 - n0 + 1, false);
+            }
+            for (int64_t n = n1; n >= n0; n--)
+                adjoint_step(A, n, tU[(size_t)(n - n0)].data(), tJU[(size_t)(n - n0)].data(),
+                             tU[(size_t)(n - n0 + 1)].data(), n >= t0 ? weight : 0.0);
+        }
+        // the first step's forces: the actuator line at t_init on U^{n_first}
+        adjoint_alm(A, t_init, Vec3<const double>{{tU[0][0], tU[0][1], tU[0][2]}}, 0.0);
+
+        // back to the end of the forward run
+        load(fin);
+        last_it = fin_last_it;
+        for (int m = 0; m < 3; m++) d2d(U[1 - ucur][m], fin_uold[m]);
+        DALM_CUDA(cudaMemcpyAsync(d_diag, fin_diag, sizeof(DiagState), cudaMemcpyDeviceToDevice, stream));
+        DALM_CUDA(cudaMemcpyAsync(d_kst, fin_kst, 2 * sizeof(KrylovState), cudaMemcpyDeviceToDevice, stream));
+        launch_alm_points(L, P, alm, fin.alm_time, c(u_cur()));
+        std::vector<double> g_dev(3 * (size_t)T);
+        DALM_CUDA(cudaMemcpyAsync(g_dev.data(), A.grad, sizeof(double) * 3 * T, cudaMemcpyDeviceToHost, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        h_kst[0] = fin_hkst[0];
+        h_kst[1] = fin_hkst[1];
+        *h_diag = fin_hdiag;
+        std::copy(fin_wt.begin(), fin_wt.end(), h_wt_out);
+        for (size_t i = 0; i < g_dev.size(); i++)
+            if (!std::isfinite(g_dev[i])) throw std::runtime_error("non-finite adjoint gradient");
+        if (grad_out) std::copy(g_dev.begin(), g_dev.end(), grad_out);
+        if (J_out) *J_out = J;
+    }
+
     void sync_stats() {
         DALM_CUDA(cudaStreamSynchronize(stream));
         if (opt.profile) harvest();
@@ -1080,13 +1377,43 @@ int dalm_set_turbine_params(dalm_handle *h, const double *yaw_deg, const double 
             d.formula[3] = yaw_deg[w] * PI_D / 180;  // deg_to_rad, src/util.h:214-216
         }
         if (omega) d.rot_speed = omega[w];
-        if (pitch_deg)
+        if (pitch_deg) {
+            h->pitch_deg[w] = pitch_deg[w];
             for (int a = w * per; a < (w + 1) * per; a++) h->twist[a] = h->base_twist[a] + pitch_deg[w];
+        }
     }
     DALM_CUDA(cudaMemcpy((void *)h->alm.wt, h->h_wt.data(), sizeof(TurbineDev) * T,
                          cudaMemcpyHostToDevice));
     DALM_CUDA(cudaMemcpy((void *)h->alm.twist, h->twist.data(), sizeof(double) * h->twist.size(),
                          cudaMemcpyHostToDevice));
+    API_END(h)
+}
+
+int dalm_get_turbine_params(dalm_handle *h, double *yaw_deg, double *pitch_deg, double *omega) {
+    API_BEGIN(h)
+    for (int w = 0; w < h->alm.wt_count; w++) {
+        const TurbineDev &d = h->h_wt[w];
+        if (yaw_deg) yaw_deg[w] = d.formula[3] * 180 / PI_D;
+        if (pitch_deg) pitch_deg[w] = h->pitch_deg[w];
+        if (omega) omega[w] = d.rot_speed;
+    }
+    API_END(h)
+}
+
+int dalm_adjoint_power_grad(dalm_handle *h, int t0, int t1, int ckpt_every, double *grad,
+                            double *J) {
+    API_BEGIN(h)
+    h->power_gradient(t0, t1, ckpt_every, grad, J);
+    API_END(h)
+}
+
+int dalm_get_adjoint_stats(dalm_handle *h, int64_t *solves, int64_t *iterations,
+                           double *max_rel_residual, int64_t *recomputed_steps) {
+    API_BEGIN(h)
+    if (solves) *solves = h->adj_stats.solves;
+    if (iterations) *iterations = h->adj_stats.iterations;
+    if (max_rel_residual) *max_rel_residual = h->adj_stats.max_rel_residual;
+    if (recomputed_steps) *recomputed_steps = h->adj_stats.recomputed_steps;
     API_END(h)
 }
 

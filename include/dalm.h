@@ -181,6 +181,34 @@ int dalm_set_inflow_profile(dalm_handle *h, const double *prof);
 int dalm_set_turbine_params(dalm_handle *h, const double *yaw_deg,
                             const double *pitch_deg, const double *omega);
 
+/* The current per-turbine parameters in the units of
+ * dalm_set_turbine_params (yaw: the angle offset in degrees). */
+int dalm_get_turbine_params(dalm_handle *h, double *yaw_deg, double *pitch_deg,
+                            double *omega);
+
+/* Discrete adjoint of the time stepping (no reference counterpart; the
+ * reference has no differentiation).  From the current state, runs the
+ * forward steps through step t1 exactly as dalm_step does (the handle ends
+ * at step t1 + 1), storing a restart point every ckpt_every steps, then the
+ * transposed steps backwards with checkpoint-every-k recomputation.
+ *   *J                 = mean over steps t0..t1 of sum_w torque_w |omega_w|
+ *   grad[3 w + 0, 1, 2] = dJ / d(yaw_deg, pitch_deg, omega) of turbine w
+ * The forces the first step reads are re-evaluated from the current velocity
+ * and parameters first (the same forces unless the parameters changed since
+ * the last actuator-line evaluation).  Requires turbines with a yaw-type
+ * angle (dalm_set_turbine_params sets it) and max(step, 1) <= t0 <= t1.
+ * The adjoint pressure solves reuse the case's solver; derivatives at the
+ * kinks (the b=4 limiter, |JU| in the upwind flux, |ft| in the torque, the
+ * polar table, trilinear cell switches) are those of the branch taken. */
+int dalm_adjoint_power_grad(dalm_handle *h, int t0, int t1, int ckpt_every,
+                            double *grad, double *J);
+
+/* Statistics of the last dalm_adjoint_power_grad: adjoint pressure solves,
+ * their total iterations, the largest final residual relative to its
+ * right-hand side, and the forward steps recomputed from restart points. */
+int dalm_get_adjoint_stats(dalm_handle *h, int64_t *solves, int64_t *iterations,
+                           double *max_rel_residual, int64_t *recomputed_steps);
+
 /* Solver::main_loop_once() x nsteps (src/solver.h:1034-1306) without field
  * output and probes; step 0 is integration-free as in the reference. */
 int dalm_step(dalm_handle *h, int nsteps);
