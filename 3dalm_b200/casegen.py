@@ -318,7 +318,7 @@ def config(name: str, **over) -> CaseSpec:
     c2  256x128x128, 1 turbine at x=4, Jacobi(3)-BiCGStab tol 1e-8
     c3  384x192x160, c2 turbine (mixed-precision case)
     c4  512x256x128, 3 turbines at x=4,9,14 yaw 0/10/0, log-law + 8%
-    c5  256x128x64,  c4 turbines (adjoint case)
+    c5  256x128x64,  c4 turbines (adjoint case; polar tabulated every 0.05 deg)
     """
     base = dict(
         c1=CaseSpec("c1", (128, 64, 64), solver="SOR", tol=1e-6, max_it=1000, relax=1.2,
@@ -332,7 +332,7 @@ def config(name: str, **over) -> CaseSpec:
                     intensity=0.08, loglaw=(0.05, 1e-3)),
         c5=CaseSpec("c5", (256, 128, 64), solver="BiCG", pc="Jacobi", pc_max_it=3, tol=1e-8,
                     max_it=10000, steps=200, turbines=_row([4.0, 9.0, 14.0], (0.0, 10.0, 0.0)),
-                    intensity=0.08, loglaw=(0.05, 1e-3)),
+                    intensity=0.08, loglaw=(0.05, 1e-3), polar_step_deg=0.05),
     )
     if name.startswith("tiny"):
         # tiny-sor / tiny-bicg / tiny-turbine / tiny-loglaw: small grids for tests

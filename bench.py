@@ -29,6 +29,7 @@ import contextlib
 import importlib
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -97,6 +98,7 @@ def parse():
                          "steps as the timed region, 0 skips it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision timing")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost run")
     return ap.parse_args()
 
 
@@ -305,6 +307,47 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ GPU side
 
+def adjoint_cost(pkg, device, steps=60, t0=31, ckpt=20):
+    """Cost of dalm_adjoint_power_grad on the 256x128x64 three-turbine case
+    (van Albada, the case's own pressure tolerance): wall time of the
+    gradient call (forward run + recomputation + reverse sweep) against the
+    same forward steps alone."""
+    cg = importlib.import_module("3dalm_b200.casegen")
+    tmp = tempfile.mkdtemp(prefix="dalm_bench_adj_")
+    spec = cg.config("c5", steps=steps)
+    mesh = cg.write_case(spec, tmp)
+    U0, prof = cg.initial_velocity(spec, mesh), cg.inflow_profile(spec, mesh)
+
+    def fresh():
+        s = pkg.Solver(tmp, device=device, limiter=pkg.VAN_ALBADA, time_average=False)
+        s.set_inflow_profile(prof)
+        s.set_state(U0)
+        s.synchronize()
+        return s
+
+    s = fresh()
+    w0 = time.perf_counter()
+    s.step(steps + 1)
+    s.synchronize()
+    fwd = time.perf_counter() - w0
+    s.finalize()
+    s = fresh()
+    w0 = time.perf_counter()
+    J, g = s.power_gradient(t0, steps, ckpt)
+    s.synchronize()
+    grad_s = time.perf_counter() - w0
+    st = s.adjoint_stats()
+    s.finalize()
+    shutil.rmtree(tmp, ignore_errors=True)
+    return {"workload": f"c5: {spec.n[0]}x{spec.n[1]}x{spec.n[2]} cells, 3 turbines, "
+                        f"steps 0..{steps}, J = mean power over steps {t0}..{steps}, "
+                        f"restart points every {ckpt} steps, van Albada",
+            "forward_s": fwd, "gradient_s": grad_s, "gradient_over_forward": grad_s / fwd,
+            "J": J, "grad_yaw_pitch_omega": g.tolist(), "adjoint_solves": st["solves"],
+            "adjoint_iterations": st["iterations"], "max_rel_residual": st["max_rel_residual"],
+            "recomputed_steps": st["recomputed_steps"], "how": "wall clock of the API calls"}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -457,6 +500,8 @@ def run_ours(args):
         "mixed": mixed,
         "clocks": clk,
     }
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_cost(pkg, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kind, desc, secs = cpu_sample("reference", statistics.mean(its))
         line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": 1, "kind": kind,

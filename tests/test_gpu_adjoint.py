@@ -129,3 +129,41 @@ def test_rejects_bad_windows(make_case):
     s2 = pkg.Solver(d)
     with pytest.raises(pkg.DalmError, match="UNSUPPORTED"):
         s2.power_gradient(1, 2, 1)
+
+
+def test_torch_autograd_function(make_case):
+    """The gradient through a torch.autograd.Function (test harness only):
+    backward returns dalm_adjoint_power_grad's gradient, checked against a
+    central difference of the Function along a random direction."""
+    torch = pytest.importorskip("torch")
+    spec, mesh, d, U0, prof = make_case("tiny-loglaw", steps=10)
+    t0, t1 = 6, 10
+
+    class MeanPower(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, params):  # (turbines, 3): yaw deg, pitch deg, rotor speed rad/s
+            p = params.detach().cpu().numpy()
+            s = solver(d, prof, U0, (p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy()))
+            J, g = s.power_gradient(t0, t1, ckpt_every=4)
+            s.close()
+            ctx.save_for_backward(torch.from_numpy(g))
+            return params.new_tensor(J)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            (g,) = ctx.saved_tensors
+            return gJ * g.to(gJ.dtype)
+
+    s0 = solver(d, prof, U0)
+    yaw, pitch, om = s0.turbine_params()
+    params = torch.tensor(np.stack([yaw, pitch, om], axis=1), dtype=torch.float64,
+                          requires_grad=True)
+    J = MeanPower.apply(params)
+    J.backward()
+    v = torch.from_numpy(np.random.default_rng(0).standard_normal(tuple(params.shape)))
+    h = 1e-5
+    with torch.no_grad():
+        dd = (MeanPower.apply(params + h * v) - MeanPower.apply(params - h * v)) / (2 * h)
+    dg = float((params.grad * v).sum())
+    print("directional derivative: autograd", dg, "central difference", float(dd))
+    assert abs(dg - float(dd)) <= 1e-5 * abs(float(dd))
