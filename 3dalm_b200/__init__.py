@@ -24,6 +24,7 @@ ERRORS = {1: "DALM_ERR_ARG", 2: "DALM_ERR_CASE", 3: "DALM_ERR_CUDA", 4: "DALM_ER
           5: "DALM_ERR_DEVICE_WAIT", 6: "DALM_ERR_UNSUPPORTED"}
 FP64, MIXED = 0, 1
 MINMOD, VAN_ALBADA = 0, 1
+INNER_MULTIGRID, INNER_BICGSTAB = 0, 1
 FIELDS = {"U": (0, 3), "Uold": (1, 3), "JU": (2, 3), "p": (3, 1), "nut": (4, 1),
           "div": (5, 1), "f": (6, 3), "b": (7, 1), "Utavg": (8, 3)}
 STAGES = {"predict": 0, "flux_rhs": 1, "poisson": 2, "project": 3, "alm": 4, "diag": 5,
@@ -56,7 +57,7 @@ class Options(C.Structure):
                 ("poisson_batch", C.c_int), ("use_graphs", C.c_int), ("profile", C.c_int),
                 ("reference_sums", C.c_int), ("fused_krylov", C.c_int),
                 ("refine_inner_it", C.c_int), ("write_output", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("mixed_inner", C.c_int), ("reserved", C.c_int * 3)]
 
 
 _PD = C.POINTER(C.c_double)
@@ -98,7 +99,8 @@ class Solver:
     def __init__(self, case_dir: str | None = None, precision: int = FP64, device: int = 0,
                  time_average: bool = True, profile: bool = False, poisson_batch: int = 0,
                  limiter: int = MINMOD, reference_sums: bool = False, fused_krylov: bool = False,
-                 refine_inner_it: int = 0, write_output: bool = False):
+                 refine_inner_it: int = 0, write_output: bool = False,
+                 mixed_inner: int = INNER_MULTIGRID):
         self.lib = load_library()
         self.h = C.c_void_p()
         self.opt = Options()
@@ -113,6 +115,7 @@ class Solver:
         self.opt.fused_krylov = int(fused_krylov)
         self.opt.refine_inner_it = int(refine_inner_it)
         self.opt.write_output = int(write_output)
+        self.opt.mixed_inner = int(mixed_inner)
         if case_dir is not None:
             self.initialize(case_dir)
 

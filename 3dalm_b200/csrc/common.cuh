@@ -258,6 +258,8 @@ enum KernelKind {
     KK_SOR_SWEEP32, KK_JACOBI_SWEEP32, KK_BICG_P32, KK_BICG_Q32, KK_BICG_S32, KK_BICG_T32, KK_BICG_XR32,
     // discrete adjoint
     KK_ADJ_BC, KK_ADJ_PROJECT, KK_ADJ_FACES, KK_ADJ_NUT, KK_ADJ_PREDICT, KK_ADJ_ALM,
+    // multigrid-preconditioned CG (inner solves of DALM_MIXED)
+    KK_MG_SMOOTH, KK_MG_TRANSFER, KK_MG_COARSE, KK_MG_PCG,
     KK_COUNT
 };
 

@@ -21,6 +21,8 @@
 #include "adjoint.cuh"
 #include "alm.cuh"
 #include "case_io.hpp"
+#include "multigrid.cuh"
+#include "multigrid_setup.hpp"
 #include "output_io.hpp"
 #include "poisson.cuh"
 
@@ -56,7 +58,7 @@ const char *kKindNames[KK_COUNT] = {
     "poisson_begin", "layout", "seq_sum", "bicg_p_fused", "bicg_s_fused", "refine_residual",
     "refine_update", "sor_sweep32", "jacobi_sweep32", "bicg_p32", "bicg_q32", "bicg_s32",
     "bicg_t32", "bicg_xr32", "adj_velocity_bc", "adj_project", "adj_faces", "adj_nut",
-    "adj_predict", "adj_alm"};
+    "adj_predict", "adj_alm", "mg_smooth", "mg_transfer", "mg_coarse", "mg_pcg"};
 
 }  // namespace
 
@@ -101,6 +103,10 @@ struct dalm_handle {
     bool mixed = false;
     long long refine_fp32_it = 0, refine_fp64_it = 0, refine_passes = 0;  // last solve
     std::vector<long long> last_inner;  // inner iterations per refinement pass, last solve
+    // multigrid-preconditioned CG inner solves (DALM_INNER_MULTIGRID)
+    bool mg_on = false;
+    MgDev mgd;
+    MgPcgBufs mgb{};
     FusedBufs fb{};
     bool fused = false;  // BiCGStab iterations as fused half-iteration kernels
     PoissonConfig pcfg{};
@@ -250,6 +256,8 @@ struct dalm_handle {
             throw std::invalid_argument("unknown precision");
         if (opt.limiter != DALM_LIMITER_MINMOD && opt.limiter != DALM_LIMITER_VAN_ALBADA)
             throw std::invalid_argument("unknown limiter");
+        if (opt.mixed_inner != DALM_INNER_MULTIGRID && opt.mixed_inner != DALM_INNER_BICGSTAB)
+            throw std::invalid_argument("unknown mixed_inner");
         const char *tr = std::getenv("DALM_TRACE_POISSON");
         trace = tr && (tr[0] == '1' || tr[0] == '2');
         trace_batches = tr && tr[0] == '2';
@@ -309,6 +317,7 @@ struct dalm_handle {
                               &pbf.pp, &pbf.ss, &pbf.tp, &pbf.ts};
             for (auto v : kv32) *v = dalloc<float>(n);
             pbf.b = pbf.r0;  // e starts at 0, so the inner r0 = r = b
+            if (opt.mixed_inner == DALM_INNER_MULTIGRID) setup_multigrid();
         }
         fb = FusedBufs{{pb.pk, nullptr}, {pb.q, nullptr}};
         if (fused) {
@@ -359,6 +368,51 @@ struct dalm_handle {
         refresh_after_state(DALM_SET_APPLY_UBC | DALM_SET_RECOMPUTE_JU, nullptr);
         DALM_CUDA(cudaStreamSynchronize(stream));
         if (opt.write_output) init_output();
+    }
+
+    // The multigrid levels of the inner solves (multigrid.cuh): merged-cell
+    // geometry from the interior centres and widths, FP32 conductances and
+    // widths, level vectors with zero guide cells, the coarsest operator's
+    // inverse.  A coarsest level above MG_MAX_COARSE cells (interior counts
+    // with large odd factors) leaves the BiCGStab inner solves in place.
+    void setup_multigrid() {
+        const int gc = (int)cs.gc;
+        const std::vector<double> *c[3] = {&cs.x, &cs.y, &cs.z}, *d[3] = {&cs.dx, &cs.dy, &cs.dz};
+        std::vector<double> cen[3], w[3];
+        for (int a = 0; a < 3; a++) {
+            cen[a].assign(c[a]->begin() + gc, c[a]->end() - gc);
+            w[a].assign(d[a]->begin() + gc, d[a]->end() - gc);
+        }
+        std::vector<MgGeometry> geo = mg_build_levels(cen, w, MG_MAX_LEVELS);
+        const MgGeometry &C = geo.back();
+        if (C.cells() > MG_MAX_COARSE) {
+            if (trace)
+                std::fprintf(stderr, "[dalm] multigrid: coarsest level %lld cells > %d, "
+                             "BiCGStab inner solves\n", C.cells(), MG_MAX_COARSE);
+            return;
+        }
+        mgd.levels = (int)geo.size();
+        for (int l = 0; l < mgd.levels; l++) {
+            const MgGeometry &G = geo[l];
+            MgLevel &v = mgd.L[l];
+            v.g = l == 0 ? g : Grid::make(G.n[0] + 2, G.n[1] + 2, G.n[2] + 2, 1);
+            for (int a = 0; a < 3; a++) {
+                v.n[a] = G.n[a];
+                v.fac[a] = G.fac[a];
+                v.cf[a] = upload(std::vector<float>(G.cf[a].begin(), G.cf[a].end()));
+                v.w[a] = upload(std::vector<float>(G.w[a].begin(), G.w[a].end()));
+            }
+            if (l > 0) {
+                mgd.x[l] = dalloc<float>((size_t)v.g.total);
+                mgd.f[l] = dalloc<float>((size_t)v.g.total);
+            }
+        }
+        std::vector<double> inv = mg_spd_inverse(mg_dense_operator(C), C.cells());
+        mgd.kinv = upload(std::vector<float>(inv.begin(), inv.end()));
+        mgd.ncoarse = (int)C.cells();
+        const size_t n = (size_t)g.total;
+        mgb = MgPcgBufs{pbf.r, pbf.x, dalloc<float>(n), dalloc<float>(n), dalloc<float>(n)};
+        mg_on = true;
     }
 
     // (Cs * cbrt(dx dy dz))^2 per interior cell with the host libm's cbrt,
@@ -505,7 +559,9 @@ struct dalm_handle {
     // one iteration n of solve `which` (0: the FP64 solve, 1: the FP32
     // inner solve of the mixed form)
     void enqueue_one(int which, long long n, KrylovState *st) {
-        if (which == 1)
+        if (which == 1 && mg_on)
+            launch_mg_iteration(L, mgd, mgb, coef.max_diag, Partials<1>{partial, ticket}, st);
+        else if (which == 1)
             launch_bicg_iteration<float>(L, g, coef, pbf, pcfg, Partials<2>{partial, ticket}, st);
         else
             enqueue_poisson_iteration(n);
@@ -601,13 +657,18 @@ struct dalm_handle {
     // that makes the residual worse is taken back; a pass that breaks down,
     // or gains less than 1/STALL, ends the refinement and the reference's
     // FP64 solve finishes from the current p.
+    // FP64 residual of the pressure, its norm and the stop test; the next
+    // inner solve's right-hand side in FP32
+    void refine_residual() {
+        launch_refine_residual(L, g, coef, pcfg, Pp, B, pbf, Partials<2>{partial, ticket}, d_kst,
+                               d_kst + 1);
+    }
     void solve_mixed() {
         const double ncell = (double)g.ni() * g.nj() * g.nk();
         const long long cap = opt.refine_inner_it > 0 ? opt.refine_inner_it : INNER_CAP;
         launch_poisson_begin(L, d_kst, max_it, tol, ncell, MAX_REFINE, INNER_RTOL, cap);
         launch_poisson_begin(L, d_kst + 1, max_it, tol, ncell, 0, 0, 0, 1);
-        launch_refine_residual(L, g, coef, pcfg, Pp, B, pbf, Partials<2>{partial, ticket}, d_kst,
-                               d_kst + 1);
+        refine_residual();
         fetch_states();
         double prev = h_kst[0].err;
         refine_fp32_it = 0;
@@ -618,6 +679,10 @@ struct dalm_handle {
         size_t pass = 0;
         while (!h_kst[0].done) {
             if (last_inner.size() <= pass) last_inner.push_back(0);
+            // multigrid-CG: scaled right-hand side, e = 0, first direction
+            // (here, not with the residual, so that a rejected pass can
+            // still take its correction back)
+            if (mg_on) launch_mg_begin(L, mgd, mgb, coef.max_diag, Partials<1>{partial, ticket}, d_kst + 1);
             last_inner[pass] = run_batches(1, last_inner[pass], cap);
             refine_fp32_it += h_kst[1].it;
             refine_passes = (long long)pass + 1;
@@ -627,8 +692,7 @@ struct dalm_handle {
                 break;
             }
             launch_refine_update(L, g, pcfg, Pp, pbf.x, 1.0);
-            launch_refine_residual(L, g, coef, pcfg, Pp, B, pbf, Partials<2>{partial, ticket},
-                                   d_kst, d_kst + 1);
+            refine_residual();
             fetch_states();
             const double now = h_kst[0].err;
             if (trace)

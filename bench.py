@@ -368,18 +368,19 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def fresh_solver(profile, precision=pkg.FP64):
+    def fresh_solver(profile, precision=pkg.FP64, inner=pkg.INNER_MULTIGRID):
         """A solver at the start of the timed steps: state set, warm-up run."""
-        sv = pkg.Solver(tmp, device=local, profile=profile, precision=precision)
+        sv = pkg.Solver(tmp, device=local, profile=profile, precision=precision,
+                        mixed_inner=inner)
         sv.set_inflow_profile(prof)
         sv.set_state(U0)
         sv.step(max(args.warmup, 1))
         return sv
 
-    def timed_region(precision):
+    def timed_region(precision, inner=pkg.INNER_MULTIGRID):
         """The K timed steps on the device (CUDA events on the solver's
         stream, no per-kernel instrumentation), max over ranks."""
-        s = fresh_solver(False, precision)
+        s = fresh_solver(False, precision, inner)
         stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
         s.timings(reset=True)
         clocks = ClockSampler(local)
@@ -420,8 +421,19 @@ def run_ours(args):
                  "max_residual": max(merrs), "fp64_max_residual": max(errs),
                  "tolerance": spec.tol, "clocks": mclk,
                  "error_vs_fp64": mixed_errors(finalm, final64),
-                 "how": "DALM_MIXED: FP64 iterative refinement with capped FP32 BiCGStab passes, "
-                        "FP64 fallback when a pass stalls; stop test on the FP64 residual"}
+                 "how": "DALM_MIXED: FP64 iterative refinement (FP64 residual, norm, pressure "
+                        "update and stop test) with capped FP32 inner passes of conjugate "
+                        "gradients preconditioned by a geometric multigrid V-cycle; FP64 "
+                        "fallback when a pass stalls. poisson_iterations counts inner CG "
+                        "iterations (one V-cycle each), not comparable with BiCGStab's"}
+        # the same form with the reference's Jacobi(3)-BiCGStab as the FP32
+        # inner solver: what precision alone gains
+        bms, bits, berrs, bclk, _, finalb = timed_region(pkg.MIXED, pkg.INNER_BICGSTAB)
+        bvalue = whole_job_rate(n_int, args.steps, world, bms / 1e3)
+        mixed["bicgstab_inner"] = {"value": bvalue, "vs_fp64": bvalue / value,
+                                   "ms_per_step": bms / args.steps, "poisson_iterations": bits,
+                                   "max_residual": max(berrs),
+                                   "error_vs_fp64": mixed_errors(finalb, final64)}
 
     # ---- end to end through the public API with host (pinned) buffers: a
     # second solver replays the same warm-up and the same timed steps, each

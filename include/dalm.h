@@ -42,12 +42,15 @@ extern "C" {
 enum dalm_precision {
     DALM_FP64 = 0,        /* every stage in FP64, the reference's arithmetic */
     DALM_MIXED = 1        /* BiCGStab pressure solve by FP64 iterative
-                             refinement with FP32 inner BiCGStab passes:
-                             residual, norms, dots and the pressure in
-                             FP64, the stop test on the FP64 residual; a
-                             pass that stalls or breaks down hands the
-                             rest of the solve to the FP64 solver.  Every
-                             other stage, and SOR / Jacobi solves, FP64. */
+                             refinement with FP32 inner passes
+                             (dalm_options.mixed_inner: multigrid-
+                             preconditioned CG by default, or the case's
+                             BiCGStab): residual, norms, dots and the
+                             pressure in FP64, the stop test on the FP64
+                             residual; a pass that stalls or breaks down
+                             hands the rest of the solve to the FP64
+                             solver.  Every other stage, and SOR / Jacobi
+                             solves, FP64.                               */
 };
 
 enum dalm_limiter {
@@ -89,6 +92,20 @@ enum dalm_stage {
 
 typedef struct dalm_handle dalm_handle;
 
+/* FP32 inner solves of DALM_MIXED (extension: the reference has FP64 only).
+ * Both stop at the same residual reduction and feed the same FP64
+ * refinement, whose stop test is the reference's. */
+enum dalm_mixed_inner {
+    DALM_INNER_MULTIGRID = 0, /* conjugate gradients preconditioned by a
+                                 geometric multigrid V-cycle (red-black
+                                 Gauss-Seidel, piecewise-constant transfers,
+                                 exact coarsest solve); falls back to
+                                 DALM_INNER_BICGSTAB when the coarsest level
+                                 would exceed 1024 cells                   */
+    DALM_INNER_BICGSTAB = 1   /* the case's Jacobi(k)-preconditioned BiCGStab
+                                 (src/eq.h:333-402) in FP32 vectors        */
+};
+
 typedef struct {
     int precision;        /* enum dalm_precision                         */
     int limiter;          /* enum dalm_limiter                           */
@@ -121,7 +138,9 @@ typedef struct {
                              output times (inst_/tavg_ binaries with U, p,
                              div, q, f / U, snapshot.json, partition.json)
                              and a per-turbine turbines.csv every step   */
-    int reserved[4];
+    int mixed_inner;      /* DALM_MIXED: the FP32 inner solver of each
+                             refinement pass, enum dalm_mixed_inner      */
+    int reserved[3];
 } dalm_options;
 
 /* Fills *opt with the defaults (FP64, minmod, device 0, time average on,

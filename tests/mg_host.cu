@@ -1,0 +1,132 @@
+// Host-side driver of the multigrid preconditioner (test infrastructure).
+//
+// Compiled by tests/test_multigrid_math.py with nvcc as host code only: it
+// builds the levels with the product's set-up code (multigrid_setup.hpp)
+// and runs the V-cycle's schedule (mg_vcycle) with the product's per-cell
+// functions (multigrid.cuh) in plain loops, so the CPU test suite can check
+// the operator against the oracle's matrix and the V-cycle's symmetry and
+// convergence.  Level 0 uses the solver's padded layout (2 guide cells).
+#include <vector>
+
+#include "../3dalm_b200/csrc/multigrid.cuh"
+#include "../3dalm_b200/csrc/multigrid_setup.hpp"
+
+using namespace dalm;
+
+namespace {
+
+struct HostMg {
+    std::vector<MgGeometry> geo;
+    std::vector<std::vector<float>> cf[3], w[3];
+    std::vector<std::vector<float>> x, f;
+    std::vector<float> kinv;
+    MgLevel L[MG_MAX_LEVELS];
+    int levels = 0, ncoarse = 0;
+
+    void smooth(int l, int color, bool zero) {
+        const MgLevel &v = L[l];
+        const long long half = (long long)v.n[0] * v.n[1] * ((v.n[2] + 1) / 2);
+        for (long long n = 0; n < half; n++) {
+            int i, j, k;
+            if (mg_color_cell(v, n, color, i, j, k))
+                mg_smooth_cell(v, x[l].data(), f[l].data(), i, j, k, zero);
+        }
+    }
+    void restrict(int l) {
+        const MgLevel &c = L[l + 1];
+        for (int I = 0; I < c.n[0]; I++)
+            for (int J = 0; J < c.n[1]; J++)
+                for (int K = 0; K < c.n[2]; K++)
+                    mg_restrict_cell(L[l], c, x[l].data(), f[l].data(), f[l + 1].data(), I, J, K);
+    }
+    void coarse() {
+        const int l = levels - 1;
+        for (int r = 0; r < ncoarse; r++) {
+            float s = 0;
+            for (int c = 0; c < ncoarse; c++)
+                s += kinv[(size_t)r * ncoarse + c] * f[l][mg_cell_index(L[l], c)];
+            x[l][mg_cell_index(L[l], r)] = s;
+        }
+    }
+    void prolong(int l) {
+        const MgLevel &v = L[l];
+        for (int i = 0; i < v.n[0]; i++)
+            for (int j = 0; j < v.n[1]; j++)
+                for (int k = 0; k < v.n[2]; k++)
+                    mg_prolong_cell(v, L[l + 1], x[l].data(), x[l + 1].data(), i, j, k);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+void *mgx_create(int n0, int n1, int n2, const double *cx, const double *cy, const double *cz,
+                 const double *wx, const double *wy, const double *wz) {
+    HostMg *m = new HostMg();
+    std::vector<double> cen[3] = {{cx, cx + n0}, {cy, cy + n1}, {cz, cz + n2}};
+    std::vector<double> w[3] = {{wx, wx + n0}, {wy, wy + n1}, {wz, wz + n2}};
+    m->geo = mg_build_levels(cen, w, MG_MAX_LEVELS);
+    m->levels = (int)m->geo.size();
+    for (int a = 0; a < 3; a++) {
+        m->cf[a].resize(m->levels);
+        m->w[a].resize(m->levels);
+    }
+    m->x.resize(m->levels);
+    m->f.resize(m->levels);
+    for (int l = 0; l < m->levels; l++) {
+        const MgGeometry &G = m->geo[l];
+        MgLevel &v = m->L[l];
+        const int gc = l == 0 ? 2 : 1;
+        v.g = Grid::make(G.n[0] + 2 * gc, G.n[1] + 2 * gc, G.n[2] + 2 * gc, gc);
+        for (int a = 0; a < 3; a++) {
+            v.n[a] = G.n[a];
+            v.fac[a] = G.fac[a];
+            m->cf[a][l].assign(G.cf[a].begin(), G.cf[a].end());
+            m->w[a][l].assign(G.w[a].begin(), G.w[a].end());
+            v.cf[a] = m->cf[a][l].data();
+            v.w[a] = m->w[a][l].data();
+        }
+        m->x[l].assign((size_t)v.g.total, 0.f);
+        m->f[l].assign((size_t)v.g.total, 0.f);
+    }
+    const MgGeometry &C = m->geo.back();
+    m->ncoarse = (int)C.cells();
+    if (m->ncoarse <= MG_MAX_COARSE) {
+        std::vector<double> inv = mg_spd_inverse(mg_dense_operator(C), C.cells());
+        m->kinv.assign(inv.begin(), inv.end());
+    }
+    return m;
+}
+
+void mgx_destroy(void *ctx) { delete (HostMg *)ctx; }
+
+int mgx_levels(void *ctx, int *out) {
+    HostMg *m = (HostMg *)ctx;
+    for (int l = 0; l < m->levels; l++)
+        for (int a = 0; a < 3; a++) out[3 * l + a] = m->L[l].n[a];
+    return m->levels;
+}
+
+long long mgx_total(void *ctx) { return ((HostMg *)ctx)->L[0].g.total; }
+
+void mgx_apply(void *ctx, const float *x, float *y) {
+    HostMg *m = (HostMg *)ctx;
+    const MgLevel &v = m->L[0];
+    for (int i = 0; i < v.n[0]; i++)
+        for (int j = 0; j < v.n[1]; j++)
+            for (int k = 0; k < v.n[2]; k++) y[v.at(i, j, k)] = mg_apply(v, x, i, j, k);
+}
+
+// x = V-cycle(f), level-0 arrays in the padded layout
+int mgx_vcycle(void *ctx, const float *f, float *x) {
+    HostMg *m = (HostMg *)ctx;
+    if (m->kinv.empty()) return -1;
+    m->f[0].assign(f, f + m->L[0].g.total);
+    std::fill(m->x[0].begin(), m->x[0].end(), 0.f);
+    mg_vcycle(*m, m->levels, MG_NU);
+    std::copy(m->x[0].begin(), m->x[0].end(), x);
+    return 0;
+}
+
+}  // extern "C"

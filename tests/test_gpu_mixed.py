@@ -2,9 +2,10 @@
 
 DALM_MIXED solves A p = b by FP64 iterative refinement: the residual
 r = b - A p, its norm and the pressure are FP64; each correction A e = r is
-an FP32 BiCGStab pass (capped); a pass that makes the FP64 residual worse is
-taken back, and one that stalls or breaks down hands the rest of the solve to
-the reference's FP64 BiCGStab.  Every solve that is not capped therefore
+an FP32 inner solve (capped): conjugate gradients preconditioned by a
+multigrid V-cycle (default) or the case's Jacobi(k)-BiCGStab; a pass that
+makes the FP64 residual worse is taken back, and one that stalls or breaks
+down hands the rest of the solve to the reference's FP64 BiCGStab.  Every solve that is not capped therefore
 ends with its residual below the case's tolerance, like the reference's, but
 at a different iterate: the pressure differs from the reference's by what two
 solutions that both meet the tolerance may differ by, and the iteration
@@ -41,10 +42,14 @@ def setup(make_case, name, precision, with_oracle=True, **kw):
     return spec, s, o
 
 
+INNER = {"multigrid": 0, "bicgstab": 1}
+
+
+@pytest.mark.parametrize("inner", sorted(INNER))
 @pytest.mark.parametrize("name", BICG)
-def test_mixed_10_steps_within_envelope(make_case, name):
+def test_mixed_10_steps_within_envelope(make_case, name, inner):
     pkg = package()
-    spec, s, o = setup(make_case, name, pkg.MIXED)
+    spec, s, o = setup(make_case, name, pkg.MIXED, mixed_inner=INNER[inner])
     worst = {"U": 0.0, "p": 0.0}
     for n in range(11):
         s.step(1)
@@ -73,9 +78,11 @@ def test_mixed_is_fp64_without_bicgstab(make_case, name):
         np.testing.assert_array_equal(a.field(f), b.field(f))
 
 
-def test_mixed_iteration_cap(make_case):
+@pytest.mark.parametrize("inner", sorted(INNER))
+def test_mixed_iteration_cap(make_case, inner):
     pkg = package()
-    spec, s, _ = setup(make_case, "tiny-bicg", pkg.MIXED, with_oracle=False, refine_inner_it=3)
+    spec, s, _ = setup(make_case, "tiny-bicg", pkg.MIXED, with_oracle=False, refine_inner_it=3,
+                       mixed_inner=INNER[inner])
     s.set_poisson(5, 0.0)
     s.step(2)
     # the cap counts FP32 and FP64 iterations together
@@ -84,7 +91,8 @@ def test_mixed_iteration_cap(make_case):
 
 def test_mixed_kernels(make_case):
     pkg = package()
-    spec, s, _ = setup(make_case, "tiny-loglaw", pkg.MIXED, with_oracle=False, profile=True)
+    spec, s, _ = setup(make_case, "tiny-loglaw", pkg.MIXED, with_oracle=False, profile=True,
+                       mixed_inner=pkg.INNER_BICGSTAB)
     s.step(3)
     kt = s.kernel_timings()
     assert kt["refine_residual"]["launches"] >= 2 * 2
@@ -93,3 +101,26 @@ def test_mixed_kernels(make_case):
     cells = int(np.prod([n - 2 * s.gc for n in s.size]))
     assert kt["bicg_q32"]["bytes_per_launch"] == 4.0 * 3 * cells
     assert kt["refine_residual"]["bytes_per_launch"] == 28.0 * cells
+
+
+def test_multigrid_inner_solves(make_case):
+    """The multigrid-CG inner solves run (their kernels launch, no BiCGStab
+    FP32 kernel does) and need a small fraction of the FP64 form's
+    iterations for the same stop test."""
+    pkg = package()
+    spec, s, _ = setup(make_case, "tiny-loglaw", pkg.MIXED, with_oracle=False, profile=True)
+    _, f, _ = setup(make_case, "tiny-loglaw", pkg.FP64, with_oracle=False)
+    its_m, its_f = [], []
+    for n in range(6):
+        s.step(1)
+        f.step(1)
+        if n >= 1:
+            its_m.append(s.stats()["it"])
+            its_f.append(f.stats()["it"])
+            assert s.stats()["err"] <= spec.tol
+    kt = s.kernel_timings()
+    print("iterations per solve: multigrid-CG", its_m, "FP64 BiCGStab", its_f)
+    assert kt["mg_smooth"]["launches"] > 0 and kt["mg_coarse"]["launches"] > 0
+    assert kt["mg_pcg"]["launches"] > 0
+    assert kt["bicg_xr32"]["launches"] == 0 and kt["jacobi_sweep32"]["launches"] == 0
+    assert sum(its_m) * 5 <= sum(its_f)
