@@ -383,7 +383,7 @@ struct dalm_handle {
             cen[a].assign(c[a]->begin() + gc, c[a]->end() - gc);
             w[a].assign(d[a]->begin() + gc, d[a]->end() - gc);
         }
-        std::vector<MgGeometry> geo = mg_build_levels(cen, w, MG_MAX_LEVELS);
+        std::vector<MgGeometry> geo = mg_build_levels(cen, w, MG_MAX_LEVELS, MG_COARSE_TARGET);
         const MgGeometry &C = geo.back();
         if (C.cells() > MG_MAX_COARSE) {
             if (trace)
@@ -406,6 +406,10 @@ struct dalm_handle {
                 mgd.x[l] = dalloc<float>((size_t)v.g.total);
                 mgd.f[l] = dalloc<float>((size_t)v.g.total);
             }
+        }
+        if (!mg_prepare(mgd)) {
+            if (trace) std::fprintf(stderr, "[dalm] multigrid: z-columns too long, BiCGStab inner solves\n");
+            return;
         }
         std::vector<double> inv = mg_spd_inverse(mg_dense_operator(C), C.cells());
         mgd.kinv = upload(std::vector<float>(inv.begin(), inv.end()));

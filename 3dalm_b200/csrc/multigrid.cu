@@ -29,15 +29,134 @@ __device__ __forceinline__ void level_loop(const MgLevel &L, F f) {
     }
 }
 
+// Zebra z-line half-sweep, one warp per column: lane l holds rows
+// k = l + 32 r (r < R, so the warp's loads and stores are coalesced rows)
+// and the tridiagonal system is solved by parallel cyclic reduction:
+// step delta combines every row with rows k -+ delta (through shuffles for
+// delta < 32, within the lane above) until each row stands alone; rows past
+// the column are identity rows.  The line operator is diagonally dominant,
+// which keeps the reduction stable without pivoting.  Same result as the
+// Thomas elimination of mg_thomas up to rounding (this file is compiled
+// with contraction and fast quotients).  Blocks only read columns
+// of the other colour and only write their own.
+template <int R>
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_smooth(MgLevel L, float *x, const float *f, int color, int zero_start,
             const KrylovState *st) {
     if (st->done) return;
-    const long long half = (long long)L.n[0] * L.n[1] * ((L.n[2] + 1) / 2);
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < half;
-         n += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        if (mg_color_cell(L, n, color, i, j, k)) mg_smooth_cell(L, x, f, i, j, k, zero_start != 0);
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long long ncol = (long long)L.n[0] * ((L.n[1] + 1) / 2);
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    const int nk = L.n[2];
+    const bool zero = zero_start != 0;
+    for (long long col = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5);
+         col < ncol; col += nw) {
+        int i, j;
+        if (!mg_color_column(L, col, color, i, j)) continue;  // uniform in the warp
+        float a[R], b[R], c[R], d[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int k = lane + 32 * r;
+            if (k < nk) {
+                float lo, hi, bb;
+                mg_zline_coef(L, i, j, k, lo, hi, bb);
+                a[r] = -lo;
+                c[r] = -hi;
+                b[r] = bb;
+                d[r] = mg_zline_rhs(L, x, f, i, j, k, zero);
+            } else {
+                a[r] = 0.f;
+                c[r] = 0.f;
+                b[r] = 1.f;
+                d[r] = 0.f;
+            }
+        }
+#pragma unroll
+        for (int delta = 1; delta < 32 * R; delta <<= 1) {
+            float na[R], nb[R], nc[R], nd[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                // row k - delta and row k + delta (identity outside the column)
+                float am = 0.f, bm = 1.f, cm = 0.f, dm = 0.f, ap = 0.f, bp = 1.f, cp = 0.f, dp = 0.f;
+                if (delta < 32) {
+                    const int src_m = (lane - delta) & 31, src_p = (lane + delta) & 31;
+                    const bool wrap_m = lane < delta, wrap_p = lane + delta >= 32;
+                    // same register r, or r - 1 / r + 1 across the lane wrap
+                    const float a0 = __shfl_sync(full, a[r], src_m), b0 = __shfl_sync(full, b[r], src_m);
+                    const float c0 = __shfl_sync(full, c[r], src_m), d0 = __shfl_sync(full, d[r], src_m);
+                    const float a1 = __shfl_sync(full, r > 0 ? a[r > 0 ? r - 1 : 0] : 0.f, src_m);
+                    const float b1 = __shfl_sync(full, r > 0 ? b[r > 0 ? r - 1 : 0] : 1.f, src_m);
+                    const float c1 = __shfl_sync(full, r > 0 ? c[r > 0 ? r - 1 : 0] : 0.f, src_m);
+                    const float d1 = __shfl_sync(full, r > 0 ? d[r > 0 ? r - 1 : 0] : 0.f, src_m);
+                    am = wrap_m ? a1 : a0; bm = wrap_m ? b1 : b0; cm = wrap_m ? c1 : c0; dm = wrap_m ? d1 : d0;
+                    const float a2 = __shfl_sync(full, a[r], src_p), b2 = __shfl_sync(full, b[r], src_p);
+                    const float c2 = __shfl_sync(full, c[r], src_p), d2 = __shfl_sync(full, d[r], src_p);
+                    const float a3 = __shfl_sync(full, r + 1 < R ? a[r + 1 < R ? r + 1 : r] : 0.f, src_p);
+                    const float b3 = __shfl_sync(full, r + 1 < R ? b[r + 1 < R ? r + 1 : r] : 1.f, src_p);
+                    const float c3 = __shfl_sync(full, r + 1 < R ? c[r + 1 < R ? r + 1 : r] : 0.f, src_p);
+                    const float d3 = __shfl_sync(full, r + 1 < R ? d[r + 1 < R ? r + 1 : r] : 0.f, src_p);
+                    ap = wrap_p ? a3 : a2; bp = wrap_p ? b3 : b2; cp = wrap_p ? c3 : c2; dp = wrap_p ? d3 : d2;
+                } else {
+                    const int m = delta / 32;
+                    if (r - m >= 0) {
+                        am = a[r - m >= 0 ? r - m : 0]; bm = b[r - m >= 0 ? r - m : 0];
+                        cm = c[r - m >= 0 ? r - m : 0]; dm = d[r - m >= 0 ? r - m : 0];
+                    }
+                    if (r + m < R) {
+                        ap = a[r + m < R ? r + m : 0]; bp = b[r + m < R ? r + m : 0];
+                        cp = c[r + m < R ? r + m : 0]; dp = d[r + m < R ? r + m : 0];
+                    }
+                }
+                // approximate quotients (2 ulp): the preconditioner needs no
+                // correctly rounded division
+                const float al = -__fdividef(a[r], bm), ga = -__fdividef(c[r], bp);
+                na[r] = al * am;
+                nc[r] = ga * cp;
+                nb[r] = b[r] + al * cm + ga * ap;
+                nd[r] = d[r] + al * dm + ga * dp;
+            }
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                a[r] = na[r];
+                b[r] = nb[r];
+                c[r] = nc[r];
+                d[r] = nd[r];
+            }
+        }
+        const long long c0 = L.at(i, j, 0);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int k = lane + 32 * r;
+            if (k < nk) x[c0 + k] = __fdividef(d[r], b[r]);
+        }
+    }
+}
+
+// longest line the warp solver takes (32 rows per register slot)
+constexpr int ZL_MAX_R = 8;
+
+template <int R>
+void zline_launch(const LaunchCtx &L, const MgLevel &v, float *x, const float *f, int color,
+                  int zero, const KrylovState *st, int blocks) {
+    k_mg_smooth<R><<<blocks, MG_THREADS, 0, L.s>>>(v, x, f, color, zero, st);
+}
+
+void zline_dispatch(const LaunchCtx &L, const MgLevel &v, float *x, const float *f, int color,
+                    int zero, const KrylovState *st) {
+    const long long ncol = (long long)v.n[0] * ((v.n[1] + 1) / 2);
+    long long nb = (ncol + MG_THREADS / 32 - 1) / (MG_THREADS / 32);
+    if (nb > L.blocks) nb = L.blocks;
+    const int R = (v.n[2] + 31) / 32;
+    switch (R) {
+    case 1: zline_launch<1>(L, v, x, f, color, zero, st, (int)nb); break;
+    case 2: zline_launch<2>(L, v, x, f, color, zero, st, (int)nb); break;
+    case 3: zline_launch<3>(L, v, x, f, color, zero, st, (int)nb); break;
+    case 4: zline_launch<4>(L, v, x, f, color, zero, st, (int)nb); break;
+    case 5: zline_launch<5>(L, v, x, f, color, zero, st, (int)nb); break;
+    case 6: zline_launch<6>(L, v, x, f, color, zero, st, (int)nb); break;
+    case 7: zline_launch<7>(L, v, x, f, color, zero, st, (int)nb); break;
+    default: zline_launch<8>(L, v, x, f, color, zero, st, (int)nb); break;
     }
 }
 
@@ -195,11 +314,8 @@ struct DeviceCycle {
     const MgDev &M;
     const KrylovState *st;
     void smooth(int l, int color, bool zero) {
-        const MgLevel &v = M.L[l];
-        const long long half = (long long)v.n[0] * v.n[1] * ((v.n[2] + 1) / 2);
         L.pre(KK_MG_SMOOTH);
-        k_mg_smooth<<<blocks_for(half, L.blocks), MG_THREADS, 0, L.s>>>(v, M.x[l], M.f[l], color,
-                                                                       zero ? 1 : 0, st);
+        zline_dispatch(L, M.L[l], M.x[l], M.f[l], color, zero ? 1 : 0, st);
         L.post(KK_MG_SMOOTH);
     }
     void restrict(int l) {
@@ -224,6 +340,12 @@ struct DeviceCycle {
 };
 
 }  // namespace
+
+bool mg_prepare(const MgDev &M) {
+    for (int l = 0; l < M.levels; l++)
+        if (M.L[l].n[2] > 32 * ZL_MAX_R) return false;
+    return true;
+}
 
 void launch_mg_vcycle(const LaunchCtx &L, const MgDev &M, const KrylovState *st) {
     DeviceCycle e{L, M, st};

@@ -10,17 +10,23 @@
 // positive definite) and f = -max_diag vol r.  Each level stores K
 // matrix-free as one conductance per face and axis (cf[a][f + 1] couples
 // cells f and f + 1 along axis a; cf[a][0] and cf[a][n] are the boundary
-// faces) and the cell widths (the face areas).  Coarser levels merge pairs
-// of cells along every axis whose count is even and at least 4 (semi-
-// coarsening where an axis can no longer halve); their operator is the same
+// faces) and the cell widths (the face areas).  The wall-stretched z
+// spacing makes the coupling strongly anisotropic, and in opposite senses
+// at the bottom (z dominates by ~400x) and the top (x, y dominate), which
+// point smoothers cannot handle; the robust combination used here is
+// z-line relaxation with semi-coarsening in x and y: coarser levels merge
+// pairs of cells along x and y while their counts are even and at least 4,
+// and along z only once neither can, down to the first level of at most
+// MG_COARSE_TARGET cells.  Each level's operator is the same
 // finite-volume Laplacian on the merged cells (centre = mean of the
 // children's centres, width = sum).  Transfers are piecewise constant: the
 // restriction sums the children's residuals (K is in integrated form), the
-// prolongation copies the coarse correction.  The smoother is red-black
-// Gauss-Seidel, pre-smoothing red then black from zero and post-smoothing
-// black then red, and the coarsest level is solved exactly with its
-// precomputed inverse: the V-cycle is a symmetric positive definite linear
-// operator, as conjugate gradients require of a preconditioner.
+// prolongation copies the coarse correction.  The smoother solves every
+// z-column exactly (zebra Gauss-Seidel over columns coloured (i + j) % 2),
+// colour 0 then 1 before the coarse correction and 1 then 0 after, and the
+// coarsest level is solved exactly with its precomputed inverse: the
+// V-cycle is a symmetric positive definite linear operator, as conjugate
+// gradients require of a preconditioner.
 //
 // Everything here is __host__ __device__ so that host-side checks run the
 // kernels' arithmetic.
@@ -34,8 +40,9 @@
 
 namespace dalm {
 
-constexpr int MG_MAX_LEVELS = 16;
-constexpr int MG_MAX_COARSE = 1024;  // cells of the coarsest level (dense inverse)
+constexpr int MG_MAX_LEVELS = 24;
+constexpr int MG_MAX_COARSE = 1024;   // cells of the coarsest level at most (dense inverse)
+constexpr int MG_COARSE_TARGET = 512;  // coarsening stops at the first level this small
 
 struct MgLevel {
     Grid g;              // storage: level 0 is the solver's grid, coarser levels gc = 1
@@ -72,38 +79,67 @@ DALM_HD float mg_apply(const MgLevel &L, const float *x, int i, int j, int k) {
     return d * x[L.at(i, j, k)] - nb;
 }
 
-DALM_HD float mg_diag(const MgLevel &L, int i, int j, int k) {
-    const float ax = L.w[1][j] * L.w[2][k], ay = L.w[0][i] * L.w[2][k],
-                az = L.w[0][i] * L.w[1][j];
-    return ax * (L.cf[0][i + 1] + L.cf[0][i]) + ay * (L.cf[1][j + 1] + L.cf[1][j]) +
-           az * (L.cf[2][k + 1] + L.cf[2][k]);
+// z-line Gauss-Seidel: column (i,j) solved exactly along k with its x and
+// y neighbours' current values on the right; columns coloured (i + j) % 2.
+// Row k of the column:  -lo x_{k-1} + b x_k - hi x_{k+1} = d_k.
+DALM_HD void mg_zline_coef(const MgLevel &L, int i, int j, int k, float &lo, float &hi,
+                           float &b) {
+    const float wi = L.w[0][i], wj = L.w[1][j];
+    const float az = wi * wj, ax = wj * L.w[2][k], ay = wi * L.w[2][k];
+    lo = az * L.cf[2][k];
+    hi = az * L.cf[2][k + 1];
+    b = ax * (L.cf[0][i + 1] + L.cf[0][i]) + ay * (L.cf[1][j + 1] + L.cf[1][j]) + lo + hi;
 }
 
-// One Gauss-Seidel update of cell (i,j,k); zero_start: the other colour is
-// still zero (the first half-sweep from x = 0 reads no neighbour).
-DALM_HD void mg_smooth_cell(const MgLevel &L, float *x, const float *f, int i, int j, int k,
-                            bool zero_start) {
+// d_k: the right-hand side plus the x and y neighbours (zero_start: they
+// are still zero)
+DALM_HD float mg_zline_rhs(const MgLevel &L, const float *x, const float *f, int i, int j, int k,
+                           bool zero_start) {
     const long long c = L.at(i, j, k);
-    if (zero_start) {
-        x[c] = f[c] / mg_diag(L, i, j, k);
-        return;
-    }
-    float d;
-    float nb = mg_neighbours(L, x, i, j, k, d);
-    x[c] = (f[c] + nb) / d;
+    if (zero_start) return f[c];
+    const float wi = L.w[0][i], wj = L.w[1][j];
+    const float ax = wj * L.w[2][k], ay = wi * L.w[2][k];
+    return f[c] + ax * (L.cf[0][i + 1] * x[c + L.g.sx] + L.cf[0][i] * x[c - L.g.sx]) +
+           ay * (L.cf[1][j + 1] * x[c + L.g.sy] + L.cf[1][j] * x[c - L.g.sy]);
 }
 
-// cell of colour `color` ((i + j + k) % 2) number n of a level: false when
-// past the end
-DALM_HD bool mg_color_cell(const MgLevel &L, long long n, int color, int &i, int &j, int &k) {
-    const int nkh = (L.n[2] + 1) / 2;
-    const long long per_i = (long long)L.n[1] * nkh;
-    if (n >= per_i * L.n[0]) return false;
-    i = (int)(n / per_i);
-    const long long r = n % per_i;
-    j = (int)(r / nkh);
-    k = 2 * (int)(r % nkh) + ((i + j + color) & 1);
-    return k < L.n[2];
+// Thomas algorithm on column (i,j): d[k * s] holds d_k on entry and x_k on
+// exit, cp[k * s] is scratch.  The rows are diagonally dominant, so the
+// elimination needs no pivoting.
+DALM_HD void mg_thomas(const MgLevel &L, int i, int j, float *d, float *cp, int s) {
+    float prev_c = 0.f, prev_d = 0.f;
+    for (int k = 0; k < L.n[2]; k++) {
+        float lo, hi, b;
+        mg_zline_coef(L, i, j, k, lo, hi, b);
+        const float m = b - lo * prev_c;
+        prev_c = hi / m;
+        prev_d = (d[k * s] + lo * prev_d) / m;
+        cp[k * s] = prev_c;
+        d[k * s] = prev_d;
+    }
+    float next = 0.f;
+    for (int k = L.n[2] - 1; k >= 0; k--) {
+        next = d[k * s] + cp[k * s] * next;
+        d[k * s] = next;
+    }
+}
+
+// the whole line update in place in x (cp: scratch of the level's layout);
+// the kernels stage the column in shared memory instead
+DALM_HD void mg_zline_column(const MgLevel &L, float *x, const float *f, float *cp, int i, int j,
+                             bool zero_start) {
+    const long long c0 = L.at(i, j, 0);
+    for (int k = 0; k < L.n[2]; k++) x[c0 + k] = mg_zline_rhs(L, x, f, i, j, k, zero_start);
+    mg_thomas(L, i, j, x + c0, cp + c0, 1);
+}
+
+// column number n of colour `color` ((i + j) % 2): false when past the end
+DALM_HD bool mg_color_column(const MgLevel &L, long long n, int color, int &i, int &j) {
+    const int njh = (L.n[1] + 1) / 2;
+    if (n >= (long long)njh * L.n[0]) return false;
+    i = (int)(n / njh);
+    j = 2 * (int)(n % njh) + ((i + color) & 1);
+    return j < L.n[1];
 }
 
 // coarse cell (I,J,K): the sum of its children's residuals f - K x
@@ -133,7 +169,8 @@ DALM_HD long long mg_cell_index(const MgLevel &L, int r) {
 }
 
 // The V-cycle's order of operations, shared by the CUDA launcher and the
-// host-side checks.  E provides smooth(level, colour, zero_start),
+// host-side checks.  E provides smooth(level, colour, zero_start) (a
+// half-sweep over the z-columns of one colour),
 // restrict(level) (f of level + 1 from level's residual), coarse() (x of
 // the last level from its f) and prolong(level) (x of level += P x of
 // level + 1).  x of level 0 = V-cycle(f of level 0).
@@ -171,6 +208,10 @@ struct MgDev {
 };
 
 struct KrylovState;
+
+// False when the levels' z-columns are longer than the line smoother takes
+// (256 cells); the mixed form then keeps its BiCGStab inner solves.
+bool mg_prepare(const MgDev &M);
 
 // x[0] = V-cycle(f[0]); every kernel returns at once when st->done is set.
 void launch_mg_vcycle(const LaunchCtx &L, const MgDev &M, const KrylovState *st);

@@ -28,24 +28,30 @@ struct MgGeometry {
     }
 };
 
-// Levels from the interior cell centres and widths of the finest grid.
+// Levels from the interior cell centres and widths of the finest grid,
+// down to the first level of at most `target` cells (solved directly).
 inline std::vector<MgGeometry> mg_build_levels(const std::vector<double> (&cen)[3],
                                                const std::vector<double> (&w)[3],
-                                               int max_levels) {
+                                               int max_levels, long long target) {
     std::vector<MgGeometry> L(1);
     for (int a = 0; a < 3; a++) {
         L[0].cen[a] = cen[a];
         L[0].w[a] = w[a];
     }
     L[0].finish();
-    while ((int)L.size() < max_levels) {
+    while ((int)L.size() < max_levels && L.back().cells() > target) {
         const MgGeometry &F = L.back();
         MgGeometry C;
         bool any = false;
-        for (int a = 0; a < 3; a++) {
-            C.fac[a] = (F.n[a] % 2 == 0 && F.n[a] >= 4) ? 2 : 1;
+        // x and y halve while they can (z-line relaxation handles z on every
+        // level); z halves only once neither x nor y can
+        auto can = [&](int a) { return F.n[a] % 2 == 0 && F.n[a] >= 4; };
+        for (int a = 0; a < 2; a++) {
+            C.fac[a] = can(a) ? 2 : 1;
             any = any || C.fac[a] == 2;
         }
+        C.fac[2] = (!any && can(2)) ? 2 : 1;
+        any = any || C.fac[2] == 2;
         if (!any) break;
         for (int a = 0; a < 3; a++) {
             for (int I = 0; I < F.n[a] / C.fac[a]; I++) {

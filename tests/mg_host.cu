@@ -23,13 +23,14 @@ struct HostMg {
     MgLevel L[MG_MAX_LEVELS];
     int levels = 0, ncoarse = 0;
 
+    std::vector<std::vector<float>> cp;
     void smooth(int l, int color, bool zero) {
         const MgLevel &v = L[l];
-        const long long half = (long long)v.n[0] * v.n[1] * ((v.n[2] + 1) / 2);
+        const long long half = (long long)v.n[0] * ((v.n[1] + 1) / 2);
         for (long long n = 0; n < half; n++) {
-            int i, j, k;
-            if (mg_color_cell(v, n, color, i, j, k))
-                mg_smooth_cell(v, x[l].data(), f[l].data(), i, j, k, zero);
+            int i, j;
+            if (mg_color_column(v, n, color, i, j))
+                mg_zline_column(v, x[l].data(), f[l].data(), cp[l].data(), i, j, zero);
         }
     }
     void restrict(int l) {
@@ -66,7 +67,7 @@ void *mgx_create(int n0, int n1, int n2, const double *cx, const double *cy, con
     HostMg *m = new HostMg();
     std::vector<double> cen[3] = {{cx, cx + n0}, {cy, cy + n1}, {cz, cz + n2}};
     std::vector<double> w[3] = {{wx, wx + n0}, {wy, wy + n1}, {wz, wz + n2}};
-    m->geo = mg_build_levels(cen, w, MG_MAX_LEVELS);
+    m->geo = mg_build_levels(cen, w, MG_MAX_LEVELS, MG_COARSE_TARGET);
     m->levels = (int)m->geo.size();
     for (int a = 0; a < 3; a++) {
         m->cf[a].resize(m->levels);
@@ -89,6 +90,7 @@ void *mgx_create(int n0, int n1, int n2, const double *cx, const double *cy, con
         }
         m->x[l].assign((size_t)v.g.total, 0.f);
         m->f[l].assign((size_t)v.g.total, 0.f);
+        m->cp.emplace_back((size_t)v.g.total, 0.f);
     }
     const MgGeometry &C = m->geo.back();
     m->ncoarse = (int)C.cells();
