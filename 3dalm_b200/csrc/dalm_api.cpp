@@ -530,7 +530,10 @@ struct dalm_handle {
     void stage_predict() {
         StageTimer t(this, DALM_STAGE_PREDICT);
         P.fbox = fbox;
-        launch_predict(L, P, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
+        if (mixed)
+            launch_predict_f32(L, P, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
+        else
+            launch_predict(L, P, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
         ucur = 1 - ucur;  // the old buffer is now Uold
     }
     void stage_flux_rhs() {
@@ -1065,6 +1068,29 @@ struct dalm_handle {
         stage_alm();
         step++;
     }
+    // The adjoint pressure solves use FP64 iterative refinement with the
+    // multigrid-CG inner solves when the case's solver is BiCGStab and the
+    // multigrid levels can be built (set up on first use in FP64 handles;
+    // a mixed handle whose inner solver is BiCGStab keeps it); the result
+    // meets the same FP64 residual test either way.
+    bool mg_tried = false;
+    bool adjoint_refinement() {
+        if (pcfg.method != PM_BICG) return false;
+        if (mixed && opt.mixed_inner != DALM_INNER_MULTIGRID) return false;
+        if (!mg_on && !mg_tried) {
+            mg_tried = true;
+            const size_t n = (size_t)g.total;
+            if (!pbf.x) {  // the refinement's FP32 vectors (multigrid path only)
+                pbf.x = dalloc<float>(n);
+                pbf.r = dalloc<float>(n);
+                pbf.r0 = dalloc<float>(n);
+                pbf.q = dalloc<float>(n);
+                pbf.b = pbf.r0;
+            }
+            setup_multigrid();
+        }
+        return mg_on;
+    }
     // A y = rhs (in B) from the guess in Pp, to an absolute RMS residual
     long long adjoint_solve(double tol_abs) {
         double ncell = (double)g.ni() * g.nj() * g.nk();
@@ -1117,7 +1143,16 @@ struct dalm_handle {
             d2d(Pp, A.y);
             launch_adj_scale(L, Pp, g.total, 1.0 / rms);
             launch_adj_scale(L, B, g.total, 1.0 / rms);
-            long long it = adjoint_solve(ADJ_RTOL);
+            long long it;
+            if (adjoint_refinement()) {
+                const double saved = tol;
+                tol = ADJ_RTOL;
+                solve_mixed();
+                tol = saved;
+                it = h_kst[0].it;
+            } else {
+                it = adjoint_solve(ADJ_RTOL);
+            }
             d2d(A.y, Pp);
             launch_adj_scale(L, A.y, g.total, rms);
             adj_stats.solves++;

@@ -86,6 +86,9 @@ __device__ inline void warp_serial_sums(const Grid &g, Term term, double (&total
 // ---- flow kernels (flow_fp64.cu) ----
 void launch_predict(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,
                     Vec3<double> unew, Vec3<const double> ju, Vec3<const double> f);
+// the mixed-precision form's predictor: the increment in FP32 (flow_mixed.cu)
+void launch_predict_f32(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,
+                        Vec3<double> unew, Vec3<const double> ju, Vec3<const double> f);
 void launch_flux_rhs(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                      Vec3<double> ju, double *b);
 void launch_flux_only(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
