@@ -59,15 +59,17 @@ def main(argv=None):
     ap.add_argument("config", nargs="?", default="c4")
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--avg-from", type=int, default=1)
+    ap.add_argument("--dt", type=float, default=None, help="override the case's time step")
     a = ap.parse_args(argv)
-    spec = casegen.config(a.config, steps=a.steps)
+    over = {"dt": a.dt} if a.dt else {}
+    spec = casegen.config(a.config, steps=a.steps, **over)
     d = tempfile.mkdtemp(prefix="dalm_mixedcheck_")
     mesh = casegen.write_case(spec, d)
     U0, prof = casegen.initial_velocity(spec, mesh), casegen.inflow_profile(spec, mesh)
     f = run(d, prof, U0, FP64, a.steps, a.avg_from)
     m = run(d, prof, U0, MIXED, a.steps, a.avg_from)
     out = {
-        "config": a.config, "cells": list(spec.n), "steps": a.steps,
+        "config": a.config, "cells": list(spec.n), "steps": a.steps, "dt": spec.dt,
         "average_over": [a.avg_from, a.steps], "tolerance": spec.tol,
         "mean_power_fp64": f["power"].tolist(), "mean_power_mixed": m["power"].tolist(),
         "mean_power_rel_diff": (np.abs(m["power"] - f["power"]) / np.abs(f["power"])).tolist(),
