@@ -176,6 +176,11 @@ class CaseSpec:
     output_start_time: float = 1e30
     output_interval_time: float = 1e30
     polar_step_deg: float = 0.5
+    # turbulence-generating grid {"bar", "mesh", "thick", "placement"}, the
+    # retracted floor's start x, probe points (the reference's own cases)
+    grid: dict | None = None
+    floor_start: float | None = None
+    probes: list = field(default_factory=list)
 
 
 def polar_tables(step_deg=0.5):
@@ -244,6 +249,12 @@ def setup_json(spec: CaseSpec, mesh: Mesh) -> dict:
         "cfd": {"Re": spec.re, "Cs": spec.cs},
         "eq": eq,
     }
+    if spec.grid is not None:
+        js["turbulence grid"] = dict(spec.grid)
+    if spec.floor_start is not None:
+        js["floor start"] = spec.floor_start
+    if spec.probes:
+        js["probe"] = [list(p) for p in spec.probes]
     if spec.turbines:
         arr = []
         for t in spec.turbines:
@@ -352,6 +363,13 @@ def config(name: str, **over) -> CaseSpec:
             spec.solver, spec.pc, spec.pc_relax = "BiCG", "SOR", 1.2
         if "jacobi" in name:
             spec.solver = "Jacobi"
+        if "tgg" in name:
+            # a turbulence-generating grid one cell thick at x = 4, a slip
+            # floor upstream of x = 3, and probes (the last one outside)
+            spec.n = (40, 20, 20)
+            spec.grid = {"bar": 0.3, "mesh": 1.0, "thick": 0.5, "placement": [4.0, 2.5, 1.5]}
+            spec.floor_start = 3.0
+            spec.probes = [[5.0, 2.5, 1.0], [7.3, 1.1, 0.4], [12.0, 3.9, 4.6], [30.0, 2.5, 1.0]]
     else:
         spec = base[name]
     for k, v in over.items():

@@ -30,6 +30,10 @@ __global__ void __launch_bounds__(256) k_adj_velocity_bc(adj::AdjBcArgs A, long 
         adj::adj_velocity_bc_column(A, n);
 }
 
+__global__ void __launch_bounds__(256) k_adj_solid(StepParams P, Vec3<double> aU, Box box) {
+    box_loop(box, [&](int i, int j, int k) { adj::adj_solid_cell(P, aU, i, j, k); });
+}
+
 __global__ void __launch_bounds__(256)
 k_adj_project(adj::AdjProjectArgs A, Box box, Partials<1> part, double *sumsq) {
     double acc = 0;
@@ -117,6 +121,14 @@ void launch_adj_project(const LaunchCtx &L, const adj::AdjProjectArgs &A, Partia
                         double *sumsq) {
     const Grid &g = A.P.g;
     Box box{{g.gc, g.gc, g.gc}, {g.nx - g.gc, g.ny - g.gc, g.nz - g.gc}};
+    if (A.P.solid) {  // the solid scaling sits between the projection and the BCs
+        L.pre(KK_ADJ_PROJECT);
+        k_adj_solid<<<L.blocks, 256, 0, L.s>>>(A.P, Vec3<double>{{const_cast<double *>(A.aU.c[0]),
+                                                                  const_cast<double *>(A.aU.c[1]),
+                                                                  const_cast<double *>(A.aU.c[2])}},
+                                                box);
+        L.post(KK_ADJ_PROJECT);
+    }
     L.pre(KK_ADJ_PROJECT);
     k_adj_project<<<L.blocks, 256, 0, L.s>>>(A, box, part, sumsq);
     L.post(KK_ADJ_PROJECT);

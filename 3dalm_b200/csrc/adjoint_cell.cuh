@@ -280,6 +280,14 @@ DALM_HD void adj_predict_cell(const AdjPredictArgs &A, int i, int j, int k) {
     }
 }
 
+// set_solid_U (src/cfd.h:1143-1160) transposed: the projected interior
+// velocity was scaled by 1 - solid
+DALM_HD void adj_solid_cell(const StepParams &P, Vec3<double> aU, int i, int j, int k) {
+    const long long c = P.g.at(i, j, k);
+    const double sf = P.solid[c];
+    for (int m = 0; m < 3; m++) aU.c[m][c] = (1. - sf) * aU.c[m][c];
+}
+
 // ---------------------------------------------- projection and Poisson
 
 // JU faces the projection changes and the next predictor reads: normal
@@ -486,8 +494,10 @@ DALM_HD void adj_velocity_bc_column(const AdjBcArgs &A, long long n) {
     lagrange3(x0, x1, x2, c[a4i], l40, l41, l42);
     for (int m = 0; m < 3; m++) {
         // the wall value equals the adjacent cell's (slip components) or 0:
-        // y-/y+ slip (v = 0), z+ slip (w = 0), z- no slip (all 0)
-        bool slip = axis == 1 ? (m != 1) : (side == 1 && m != 2);
+        // y-/y+ slip (v = 0), z+ slip (w = 0), z- no slip (all 0) or slip
+        // upstream of a retracted floor's start
+        bool slip = axis == 1 ? (m != 1)
+                              : ((side == 1 || (P.retracted && P.m.x[i] < P.floor_start)) && m != 2);
         double g3 = A.aU.c[m][a3], g4 = A.aU.c[m][a4];
         A.aU.c[m][a0] += l30 * g3 + l40 * g4;
         A.aU.c[m][a1] += (l31 + (slip ? l32 : 0.0)) * g3 + (l41 + (slip ? l42 : 0.0)) * g4;

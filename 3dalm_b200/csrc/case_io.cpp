@@ -121,10 +121,23 @@ CaseData load_case(const std::string &dir) {
     c.tavg_start_time = setup["output"]["time avg start time"].number();
     c.output_start_time = setup["output"]["output start time"].number();
     c.output_interval_time = setup["output"]["output interval time"].number();
-    if (setup.contains("turbulence grid"))
-        throw std::runtime_error("setup.json: \"turbulence grid\" is not supported by this build");
-    if (setup.contains("floor start"))
-        throw std::runtime_error("setup.json: \"floor start\" (retracted floor) is not supported by this build");
+    if (setup.contains("turbulence grid")) {  // src/solver.h:599-611
+        const Json &tg = setup["turbulence grid"];
+        c.has_grid = true;
+        c.grid_thick = tg["thick"].number();
+        c.grid_mesh = tg["mesh"].number();
+        c.grid_bar = tg["bar"].number();
+        for (int m = 0; m < 3; m++) c.grid_at[m] = tg["placement"][m].number();
+    }
+    if (setup.contains("floor start")) {  // src/solver.h:618-625
+        c.retracted_floor = true;
+        c.floor_start = setup["floor start"].number();
+    }
+    if (setup.contains("probe")) {  // src/solver.h:656-664
+        const Json &pr = setup["probe"];
+        for (size_t m = 0; m < pr.size(); m++)
+            for (int a = 0; a < 3; a++) c.probes.push_back(pr[m][a].number());
+    }
 
     // inflow / cfd (src/solver.h:627-635)
     for (int m = 0; m < 3; m++) c.uin[m] = setup["inflow"]["value"][m].number();

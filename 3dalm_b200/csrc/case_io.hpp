@@ -32,6 +32,15 @@ struct CaseData {
     int64_t max_it = 0, pc_max_it = 0;
     double tol = 0, relax = 1, pc_relax = 1;
     double max_diag = 0;
+    // turbulence-generating grid (src/solver.h:599-611): bar width, mesh
+    // spacing, thickness, placement
+    bool has_grid = false;
+    double grid_bar = 0, grid_mesh = 0, grid_thick = 0, grid_at[3] = {0, 0, 0};
+    // retracted floor (src/solver.h:618-625): slip z- wall for x < floor_start
+    bool retracted_floor = false;
+    double floor_start = 0;
+    // probes (src/solver.h:656-699): requested points
+    std::vector<double> probes;  // [n][3]
     // actuator line
     int64_t blades = 0, ap_per_blade = 0, atk_count = 0;
     double projection_width = 0;

@@ -153,6 +153,9 @@ struct dalm_handle {
 
     void release() {
         if (stream) cudaStreamSynchronize(stream);
+        for (auto &p : probe_list)
+            if (!p.recs.empty()) flush_probe(p);
+        probe_list.clear();
         for (auto &gu : graph_unit) {
             if (gu.exec) cudaGraphExecDestroy(gu.exec);
             gu.exec = nullptr;
@@ -358,6 +361,13 @@ struct dalm_handle {
         P.reference_sums = opt.reference_sums ? 1 : 0;
         P.limiter = opt.limiter == DALM_LIMITER_VAN_ALBADA ? 1 : 0;
         P.filter2 = build_filter();
+        P.solid = nullptr;
+        P.retracted = cs.retracted_floor ? 1 : 0;
+        P.floor_start = cs.floor_start;
+        if (cs.has_grid) {
+            solid_host = build_solid();
+            P.solid = upload(solid_host);
+        }
 
         init_alm();
 
@@ -365,6 +375,14 @@ struct dalm_handle {
         // p = 0, BCs, flux, nut/div (on demand here), ALM force, diagnostics.
         for (int b = 0; b < 2; b++)
             for (int m = 0; m < 3; m++) launch_fill(L, U[b][m], g.total, cs.uin[m]);
+        if (cs.has_grid) {  // set_solid_U on the initial field (src/solver.h:767-770)
+            std::vector<double> u((size_t)g.total);
+            for (int m = 0; m < 3; m++) {
+                for (size_t c = 0; c < u.size(); c++) u[c] = (1. - solid_host[c]) * cs.uin[m];
+                DALM_CUDA(cudaMemcpy(U[ucur][m], u.data(), sizeof(double) * u.size(),
+                                     cudaMemcpyHostToDevice));
+            }
+        }
         refresh_after_state(DALM_SET_APPLY_UBC | DALM_SET_RECOMPUTE_JU, nullptr);
         DALM_CUDA(cudaStreamSynchronize(stream));
         if (opt.write_output) init_output();
@@ -417,6 +435,42 @@ struct dalm_handle {
         const size_t n = (size_t)g.total;
         mgb = MgPcgBufs{pbf.r, pbf.x, dalloc<float>(n), dalloc<float>(n), dalloc<float>(n)};
         mg_on = true;
+    }
+
+    // Solid volume fraction of the turbulence-generating grid per interior
+    // cell (set_turbulence_generating_grid, src/solver.h:52-159): a vertical
+    // bar layer of thickness `thick` ending at x = placement_x, with bars of
+    // width `bar` every `mesh` in y, and a horizontal bar layer just upstream
+    // with bars every `mesh` in z; same operation order as the reference.
+    std::vector<double> solid_host;
+    static double intersection(double h1, double t1, double h2, double t2) {
+        double l1 = t1 - h1, l2 = t2 - h2, x1 = t1 - h2, x2 = t2 - h1;  // src/util.h:84-90
+        return std::fmax(0., std::fmin(l1, std::fmin(l2, std::fmin(x1, x2))));
+    }
+    std::vector<double> build_solid() const {
+        std::vector<double> s((size_t)g.total, 0.0);
+        const double thick = cs.grid_thick, mesh_w = cs.grid_mesh, bar = cs.grid_bar;
+        const double gx = cs.grid_at[0], gy = cs.grid_at[1], gz = cs.grid_at[2];
+        for (int i = g.gc; i < g.nx - g.gc; i++)
+            for (int j = g.gc; j < g.ny - g.gc; j++)
+                for (int k = g.gc; k < g.nz - g.gc; k++) {
+                    double xc = cs.x[i], yc = cs.y[j], zc = cs.z[k];
+                    double dxc = cs.dx[i], dyc = cs.dy[j], dzc = cs.dz[k];
+                    double xv = intersection(xc - 0.5 * dxc, xc + 0.5 * dxc, gx - thick, gx);
+                    int64_t bj = (int64_t)std::round((yc - gy) / mesh_w);
+                    double by = bj * mesh_w + gy;
+                    double yi = intersection(yc - 0.5 * dyc, yc + 0.5 * dyc, by - 0.5 * bar,
+                                             by + 0.5 * bar);
+                    double xh = intersection(xc - 0.5 * dxc, xc + 0.5 * dxc, gx - 2 * thick,
+                                             gx - thick);
+                    int64_t bk = (int64_t)std::round((zc - gz) / mesh_w);
+                    double bz = bk * mesh_w + gz;
+                    double zi = intersection(zc - 0.5 * dzc, zc + 0.5 * dzc, bz - 0.5 * bar,
+                                             bz + 0.5 * bar);
+                    double occupied = xv * yi * dzc + xh * zi * dyc;
+                    s[(size_t)g.at(i, j, k)] = occupied / (dxc * dyc * dzc);
+                }
+        return s;
     }
 
     // (Cs * cbrt(dx dy dz))^2 per interior cell with the host libm's cbrt,
@@ -854,12 +908,91 @@ struct dalm_handle {
                 turbine_log << ",thrust" << w << ",torque" << w << ",power" << w;
             turbine_log << "\n";
         }
+        if (cs.has_grid) {  // the grid's solid fraction at set-up (src/solver.h:747-762)
+            std::vector<double> ref((size_t)cs.size[0] * cs.size[1] * cs.size[2], 0.0);
+            for (int i = 0; i < g.nx; i++)
+                for (int j = 0; j < g.ny; j++)
+                    for (int k = 0; k < g.nz; k++)
+                        ref[((size_t)i * g.ny + j) * g.nz + k] = solid_host[(size_t)g.at(i, j, k)];
+            write_field_binary(out_dir + "/" + binary_filename("solid", 0, step), cs.size, cs.gc,
+                               cs.x, cs.y, cs.z, {{"solid", 1, ref.data()}});
+        }
+        init_probes();
+    }
+
+    // ---- probes (struct Probe, src/solver.h:406-465) ----------------------
+    // Each requested point is snapped to the nearest cell centre among the
+    // interior and the first guide layer (find_nearest_index, src/util.h:
+    // 92-106); points that land in the guide layer stay inactive.  Active
+    // probes record (t, u, v, w) in FP32 every step once t >= output start
+    // time, buffered and appended to probe<m>.csv every 10000 records and
+    // when the handle is destroyed, in the reference's text format.
+    struct Probe {
+        std::string path;
+        long long cell;  // device index
+        std::vector<std::array<float, 4>> recs;
+    };
+    std::vector<Probe> probe_list;
+    long long *d_probe_idx = nullptr;
+    double *d_probe_val = nullptr;
+    static int64_t nearest_index(const double *x, double y, int64_t len) {
+        if (y < x[0]) return 0;
+        if (y >= x[len - 1]) return len - 1;
+        for (int64_t i = 0; i < len - 1; i++)
+            if (x[i] <= y && y < x[i + 1]) return (y - x[i] < x[i + 1] - y) ? i : i + 1;
+        return -1;
+    }
+    void init_probes() {
+        const int64_t gc = cs.gc;
+        std::vector<long long> idx;
+        for (size_t m = 0; 3 * m + 2 < cs.probes.size(); m++) {
+            const double px = cs.probes[3 * m], py = cs.probes[3 * m + 1], pz = cs.probes[3 * m + 2];
+            int64_t ni = nearest_index(cs.x.data() + gc - 1, px, cs.size[0] - 2 * gc + 2) + gc - 1;
+            int64_t nj = nearest_index(cs.y.data() + gc - 1, py, cs.size[1] - 2 * gc + 2) + gc - 1;
+            int64_t nk = nearest_index(cs.z.data() + gc - 1, pz, cs.size[2] - 2 * gc + 2) + gc - 1;
+            if (!(ni >= gc && ni < cs.size[0] - gc && nj >= gc && nj < cs.size[1] - gc && nk >= gc &&
+                  nk < cs.size[2] - gc))
+                continue;
+            Probe p;
+            p.path = out_dir + "/probe" + std::to_string(m) + ".csv";
+            p.cell = g.at((int)ni, (int)nj, (int)nk);
+            std::ofstream ofs(p.path);
+            if (!ofs) throw std::runtime_error("cannot write " + p.path);
+            ofs << "# " << cs.x[ni] << " " << cs.y[nj] << " " << cs.z[nk] << std::endl;
+            ofs << "t,u,v,w" << std::endl;
+            idx.push_back(p.cell);
+            probe_list.push_back(std::move(p));
+        }
+        if (!idx.empty()) {
+            d_probe_idx = upload(idx);
+            d_probe_val = dalloc<double>(3 * idx.size());
+        }
+    }
+    void record_probes(double t) {
+        if (probe_list.empty() || !(t >= cs.output_start_time)) return;
+        const int n = (int)probe_list.size();
+        std::vector<double> v(3 * (size_t)n);
+        launch_gather_points(L, c(u_cur()), d_probe_idx, n, d_probe_val);
+        DALM_CUDA(cudaMemcpyAsync(v.data(), d_probe_val, sizeof(double) * v.size(),
+                                  cudaMemcpyDeviceToHost, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        for (int m = 0; m < n; m++) {
+            Probe &p = probe_list[m];
+            p.recs.push_back({(float)t, (float)v[3 * m], (float)v[3 * m + 1], (float)v[3 * m + 2]});
+            if (p.recs.size() == 10000) flush_probe(p);
+        }
+    }
+    static void flush_probe(Probe &p) {
+        std::ofstream ofs(p.path, std::ios::app);
+        for (const auto &r : p.recs) ofs << r[0] << "," << r[1] << "," << r[2] << "," << r[3] << std::endl;
+        p.recs.clear();
     }
     // The end of main_loop_once (src/solver.h:1194-1253): the turbine loads,
     // and at the output times the inst_ file (U, p, div, q, f), the tavg_
     // file (time-averaged U) once averaging has started, and snapshot.json.
     void write_outputs() {
         const double t = cs.dt * (double)step;
+        record_probes(t);
         if (turbine_log.is_open() && step != 0) {
             sync_stats();
             char buf[96];

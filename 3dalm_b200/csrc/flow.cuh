@@ -44,6 +44,12 @@ struct StepParams {
     // (warp_serial_sums) instead of the parallel tree
     int reference_sums;
     int limiter;  // 0: the reference's b=4 limiter, 1: van Albada
+    // turbulence-generating grid: solid volume fraction per cell (null: none);
+    // set_solid_U scales the projected velocity by 1 - solid
+    const double *solid;
+    // retracted floor: the z- wall is slip for cell centres x < floor_start
+    int retracted;
+    double floor_start;
 };
 
 struct DiagState {
@@ -113,5 +119,8 @@ void launch_to_device_layout(const LaunchCtx &L, const Grid &g, const double *re
 void launch_to_ref_layout(const LaunchCtx &L, const Grid &g, double *const *src, int ncomp,
                           double *ref);
 void launch_fill(const LaunchCtx &L, double *p, long long n, double v);
+// out[3 t + m] = U_m at device index idx[t] (probe sampling)
+void launch_gather_points(const LaunchCtx &L, Vec3<const double> u, const long long *idx, int n,
+                          double *out);
 
 }  // namespace dalm

@@ -287,7 +287,7 @@ __device__ __forceinline__ double proj_face(const StepParams &P, Vec3<double> JU
     }
 }
 
-// project_p (src/cfd.h:601-783) + the apply_JUbc that follows it
+// project_p (src/cfd.h:601-783) + set_solid_U + the apply_JUbc that follows it
 // + calc_divergence norm + calc_max_cfl (src/solver.h:1122-1186).  The
 // velocity BCs (apply_Ubc) run in k_velocity_bc after this kernel; they touch
 // guide cells only, so the interior velocity used for the CFL here is final.
@@ -315,6 +315,12 @@ k_project(StepParams P, Segments T, Vec3<double> U, Vec3<double> JUin, Vec3<doub
             double v = U.c[1][c] - P.dt * (p[g.at(i, j + 1, k)] - p[g.at(i, j - 1, k)]) /
                                        (P.m.y[j + 1] - P.m.y[j - 1]);
             double w = U.c[2][c] - P.dt * (p[c + 1] - p[c - 1]) / (P.m.z[k + 1] - P.m.z[k - 1]);
+            if (P.solid) {  // set_solid_U (src/cfd.h:1143-1160)
+                const double sf = P.solid[c];
+                u = (1. - sf) * u;
+                v = (1. - sf) * v;
+                w = (1. - sf) * w;
+            }
             U.c[0][c] = u;
             U.c[1][c] = v;
             U.c[2][c] = w;
@@ -489,7 +495,9 @@ __global__ void k_velocity_bc(StepParams P, Vec3<double> U, Vec3<const double> V
         double z2 = side ? P.m.z[k1] + 0.5 * P.m.dz[k1] : P.m.z[k1] - 0.5 * P.m.dz[k1];
         double z3 = P.m.z[k3], z4 = P.m.z[k4];
         double ubc[3] = {0, 0, 0};
-        if (side) {
+        // z+ slip; z- no slip, or slip upstream of a retracted floor's start
+        // (src/bc.h:140-160)
+        if (side || (P.retracted && P.m.x[i] < P.floor_start)) {
             ubc[0] = U.c[0][a1];
             ubc[1] = U.c[1][a1];
         }
@@ -618,6 +626,12 @@ int plane_blocks(const Grid &g) {
     return (int)(b < 4096 ? (b > 0 ? b : 1) : 4096);
 }
 
+__global__ void k_gather_points(Vec3<const double> U, const long long *idx, int n, double *out) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    for (int m = 0; m < 3; m++) out[3 * t + m] = U.c[m][idx[t]];
+}
+
 }  // namespace
 
 void launch_predict(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,
@@ -724,6 +738,14 @@ void launch_to_ref_layout(const LaunchCtx &L, const Grid &g, double *const *src,
     L.pre(KK_LAYOUT);
     k_to_ref<<<L.blocks, 256, 0, L.s>>>(g, src[0], ncomp == 3 ? src[1] : nullptr,
                                         ncomp == 3 ? src[2] : nullptr, ncomp, ref);
+    L.post(KK_LAYOUT);
+}
+
+void launch_gather_points(const LaunchCtx &L, Vec3<const double> u, const long long *idx, int n,
+                          double *out) {
+    if (n <= 0) return;
+    L.pre(KK_LAYOUT);
+    k_gather_points<<<(n + 127) / 128, 128, 0, L.s>>>(u, idx, n, out);
     L.post(KK_LAYOUT);
 }
 

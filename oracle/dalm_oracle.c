@@ -46,6 +46,9 @@ struct dalm_oracle {
     double avg_div, max_cfl;
     int sum_order; /* 0: the reference's serial sums; 1: pairwise (test only) */
     int limiter;   /* 0: the reference's b=4 limiter, 1: van Albada (extension) */
+    double *solid; /* turbulence-generating grid's solid fraction, or NULL */
+    int retracted; /* retracted floor */
+    double floor_start;
     /* runtime (src/solver.h:176-205) */
     int64_t step, max_step, tavg_count;
     double tavg_start_time;
@@ -101,6 +104,46 @@ static void build_spacing(const double *c, double *d, int64_t n) {
     for (int64_t i = 1; i < n - 1; i++) d[i] = 0.5 * (c[i + 1] - c[i - 1]);
     d[0] = -1.5 * c[0] + 2.0 * c[1] - 0.5 * c[2];
     d[n - 1] = 1.5 * c[n - 1] - 2.0 * c[n - 2] + 0.5 * c[n - 3];
+}
+
+/* get_intersection, src/util.h:84-90 */
+static double intersection(double h1, double t1, double h2, double t2) {
+    double l1 = t1 - h1, l2 = t2 - h2, x1 = t1 - h2, x2 = t2 - h1;
+    return fmax(0., fmin(l1, fmin(l2, fmin(x1, x2))));
+}
+
+/* set_turbulence_generating_grid, src/solver.h:52-159 */
+static void build_solid(dalm_oracle *o, const oracle_params *prm) {
+    o->solid = calloc(o->len, sizeof(double));
+    double thick = prm->grid_thick, mesh = prm->grid_mesh, bar = prm->grid_bar;
+    double gx = prm->grid_at[0], gy = prm->grid_at[1], gz = prm->grid_at[2];
+    for (int64_t i = o->gc; i < o->nx - o->gc; i++)
+        for (int64_t j = o->gc; j < o->ny - o->gc; j++)
+            for (int64_t k = o->gc; k < o->nz - o->gc; k++) {
+                double xc = o->x[i], yc = o->y[j], zc = o->z[k];
+                double dxc = o->dx[i], dyc = o->dy[j], dzc = o->dz[k];
+                double xv = intersection(xc - 0.5 * dxc, xc + 0.5 * dxc, gx - thick, gx);
+                int64_t bj = (int64_t)round((yc - gy) / mesh);
+                double by = bj * mesh + gy;
+                double yi = intersection(yc - 0.5 * dyc, yc + 0.5 * dyc, by - 0.5 * bar, by + 0.5 * bar);
+                double xh = intersection(xc - 0.5 * dxc, xc + 0.5 * dxc, gx - 2 * thick, gx - thick);
+                int64_t bk = (int64_t)round((zc - gz) / mesh);
+                double bz = bk * mesh + gz;
+                double zi = intersection(zc - 0.5 * dzc, zc + 0.5 * dzc, bz - 0.5 * bar, bz + 0.5 * bar);
+                double occupied = xv * yi * dzc + xh * zi * dyc;
+                o->solid[ID(o, i, j, k)] = occupied / (dxc * dyc * dzc);
+            }
+}
+
+/* set_solid_U, src/cfd.h:1143-1160 */
+static void solid_velocity(dalm_oracle *o) {
+    if (!o->solid) return;
+    for (int64_t i = o->gc; i < o->nx - o->gc; i++)
+        for (int64_t j = o->gc; j < o->ny - o->gc; j++)
+            for (int64_t k = o->gc; k < o->nz - o->gc; k++) {
+                int64_t id = ID(o, i, j, k);
+                for (int m = 0; m < 3; m++) o->U[id * 3 + m] = (1. - o->solid[id]) * o->U[id * 3 + m];
+            }
 }
 
 /* build_A, src/eq.h:701-798 (single domain, offset 0) */
@@ -213,6 +256,12 @@ dalm_oracle *oracle_create(const oracle_params *prm) {
     /* fill U, Uold with Uin, p = 0: src/solver.h:737-740 */
     for (int64_t id = 0; id < L; id++)
         for (int m = 0; m < 3; m++) o->U[id * 3 + m] = o->Uold[id * 3 + m] = o->uin[m];
+    o->retracted = prm->retracted_floor;
+    o->floor_start = prm->floor_start;
+    if (prm->has_grid) {  /* src/solver.h:742-770 */
+        build_solid(o, prm);
+        solid_velocity(o);
+    }
     /* turbines: build_wt_props, src/alm.h:144-206 (angle slots parsed by caller) */
     o->wt_count = prm->turbine_count;
     o->blades = prm->blades;
@@ -238,7 +287,7 @@ void oracle_destroy(dalm_oracle *o) {
     double *all[] = {o->x, o->y, o->z, o->dx, o->dy, o->dz, o->U, o->Uold, o->Utavg, o->JU,
                      o->p, o->nut, o->div, o->f, o->A, o->b, o->r, o->r0, o->pk, o->pp,
                      o->q, o->s, o->ss, o->t, o->tmp, o->profile, o->base_twist, o->cd,
-                     o->cl, o->atk};
+                     o->cl, o->atk, o->solid};
     for (size_t a = 0; a < sizeof(all) / sizeof(all[0]); a++) free(all[a]);
     free(o->wt);
     free(o->ap);
@@ -679,7 +728,11 @@ static void velocity_bc(dalm_oracle *o) {
                 double z2 = side ? o->z[k1] + 0.5 * o->dz[k1] : o->z[k1] - 0.5 * o->dz[k1];
                 double z3 = o->z[k3], z4 = o->z[k4];
                 double ubc[3] = {0, 0, 0};
-                if (side) { ubc[0] = U[a1 * 3 + 0]; ubc[1] = U[a1 * 3 + 1]; }
+                /* z+ slip; z- no slip, or slip upstream of a retracted floor (src/bc.h:140-160) */
+                if (side || (o->retracted && o->x[i] < o->floor_start)) {
+                    ubc[0] = U[a1 * 3 + 0];
+                    ubc[1] = U[a1 * 3 + 1];
+                }
                 for (int m = 0; m < 3; m++) {
                     double f0 = U[a0 * 3 + m], f1 = U[a1 * 3 + m], f2 = ubc[m];
                     U[a3 * 3 + m] = quad_poly(z0, z1, z2, f0, f1, f2, z3);
@@ -915,6 +968,7 @@ void oracle_stage(dalm_oracle *o, int stage) {
     case 3:
         pressure_bc(o);
         project(o);
+        solid_velocity(o);
         velocity_bc(o);
         flux_bc(o);
         eddy_viscosity(o);

@@ -51,6 +51,13 @@ typedef struct {
     const double *station_r, *station_chord, *station_twist; /* [S] */
     const double *station_cd, *station_cl;                   /* [S][atk] */
     const double *atk;                                       /* [atk] */
+    /* turbulence-generating grid (has_grid != 0): bar width, mesh spacing,
+     * thickness, placement (src/solver.h:599-611) */
+    int has_grid;
+    double grid_bar, grid_mesh, grid_thick, grid_at[3];
+    /* retracted floor: slip z- wall for x < floor_start (src/solver.h:618-625) */
+    int retracted_floor;
+    double floor_start;
 } oracle_params;
 
 typedef struct dalm_oracle dalm_oracle;

@@ -109,6 +109,9 @@ class Case:
         self.pc = pc.get("method", "Jacobi")
         self.pc_max_it = int(pc.get("max iteration", 0))
         self.pc_relax = float(pc.get("relaxation rate", 1.0))
+        # turbulence-generating grid and retracted floor (src/solver.h:599-625)
+        self.grid = s.get("turbulence grid")
+        self.floor_start = s.get("floor start")
         self.turbines = []
         self.wt = None
         if "windturbine array" in s:
@@ -143,6 +146,15 @@ class Case:
         P.pc = PCS[self.pc]
         P.max_it, P.pc_max_it = self.max_it, self.pc_max_it
         P.tol, P.relax, P.pc_relax = self.tol, self.relax, self.pc_relax
+        if self.grid is not None:
+            P.has_grid = 1
+            P.grid_bar = float(self.grid["bar"])
+            P.grid_mesh = float(self.grid["mesh"])
+            P.grid_thick = float(self.grid["thick"])
+            P.grid_at = (C.c_double * 3)(*[float(v) for v in self.grid["placement"]])
+        if self.floor_start is not None:
+            P.retracted_floor = 1
+            P.floor_start = float(self.floor_start)
         if self.turbines:
             wt = self.wt
             P.turbine_count = len(self.turbines)
@@ -185,6 +197,9 @@ class OracleParams(C.Structure):
         ("station_count", C.c_int64), ("atk_count", C.c_int64),
         ("station_r", _PD), ("station_chord", _PD), ("station_twist", _PD),
         ("station_cd", _PD), ("station_cl", _PD), ("atk", _PD),
+        ("has_grid", C.c_int), ("grid_bar", C.c_double), ("grid_mesh", C.c_double),
+        ("grid_thick", C.c_double), ("grid_at", C.c_double * 3),
+        ("retracted_floor", C.c_int), ("floor_start", C.c_double),
     ]
 
 

@@ -60,16 +60,16 @@ def test_bad_case_reports_case_error(lib, tmp_path):
     assert b"JSON" in lib.dalm_last_error(None)
 
 
-def test_unsupported_case_features_rejected(lib, make_case):
+def test_incomplete_turbulence_grid_rejected(lib, make_case):
     spec, mesh, d, U0, prof = make_case("tiny-sor")
     with open(os.path.join(d, "setup.json")) as f:
         s = json.load(f)
-    s["turbulence grid"] = {"bar": 0.1, "mesh": 0.4, "thick": 0.06, "placement": [1, 1, 1]}
+    s["turbulence grid"] = {"bar": 0.1, "thick": 0.06, "placement": [1, 1, 1]}  # no "mesh"
     with open(os.path.join(d, "setup.json"), "w") as f:
         json.dump(s, f)
     h = C.c_void_p()
     assert lib.dalm_create(d.encode(), None, C.byref(h)) == 2
-    assert b"turbulence grid" in lib.dalm_last_error(None)
+    assert b"mesh" in lib.dalm_last_error(None)
 
 
 def test_valid_case_without_gpu_reports_cuda_error(lib, make_case):

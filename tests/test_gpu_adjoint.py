@@ -167,3 +167,27 @@ def test_torch_autograd_function(make_case):
     dg = float((params.grad * v).sum())
     print("directional derivative: autograd", dg, "central difference", float(dd))
     assert abs(dg - float(dd)) <= 1e-5 * abs(float(dd))
+
+
+def test_gradient_with_grid_and_floor(make_case):
+    """The transposed solid scaling and retracted-floor wall: a
+    turbulence-generating grid upstream of the rotors and a slip floor up to
+    x = 2, against central differences."""
+    grid = {"bar": 0.4, "mesh": 1.25, "thick": 0.5, "placement": [2.5, 2.5, 1.5]}
+    spec, mesh, d, U0, prof = make_case("tiny-loglaw", steps=12, grid=grid, floor_start=2.0)
+    t0, t1 = 7, 12
+    s = solver(d, prof, U0)
+    base = s.turbine_params()
+    J, g = s.power_gradient(t0, t1, ckpt_every=4)
+    h = 1e-5
+    fd = np.zeros_like(g)
+    for w in range(g.shape[0]):
+        for q in range(3):
+            pp = [v.copy() for v in base]
+            pm = [v.copy() for v in base]
+            pp[q][w] += h
+            pm[q][w] -= h
+            fd[w, q] = (objective(d, prof, U0, pp, t0, t1) -
+                        objective(d, prof, U0, pm, t0, t1)) / (2 * h)
+    print("adjoint\n", g, "\nfinite differences\n", fd, "\nrelative", np.abs(g - fd) / np.abs(fd))
+    assert np.all(np.abs(g - fd) <= 1e-4 * np.abs(fd) + 1e-7 * np.abs(fd).max())

@@ -96,3 +96,20 @@ def test_outputs_with_turbines(make_case, tmp_path):
     assert len(rows) == 1 + spec.steps
     last = [float(v) for v in rows[-1].split(",")]
     assert last[0] == spec.steps and last[2] > 0
+
+
+def test_outputs_with_grid_floor_and_probes(make_case, tmp_path):
+    """A turbulence-generating grid, a retracted floor and probes (the
+    reference's own cases use all three): every output file, including
+    solid_* and probe*.csv, byte-identical to the reference solver's."""
+    spec, ours, ref = run_both(make_case, tmp_path, "tiny-tgg", reference_sums=True)
+    names = sorted(os.listdir(ref))
+    assert "solid_00000_0000000000" in names
+    assert [n for n in names if n.startswith("probe")] == ["probe0.csv", "probe1.csv", "probe2.csv"]
+    assert names == sorted(os.listdir(ours))
+    for n in names:
+        a, b = os.path.join(ours, n), os.path.join(ref, n)
+        if n.endswith(".json"):
+            assert json.load(open(a)) == json.load(open(b)), n
+        else:
+            assert open(a, "rb").read() == open(b, "rb").read(), n

@@ -30,7 +30,7 @@ from test_oracle_sensitivity import ENVELOPE
 
 pytestmark = pytest.mark.gpu
 
-NO_TURBINE = ["tiny-sor", "tiny-bicg", "tiny-sorpc", "tiny-jacobi"]
+NO_TURBINE = ["tiny-sor", "tiny-bicg", "tiny-sorpc", "tiny-jacobi", "tiny-tgg"]
 TURBINE = ["tiny-turbine", "tiny-loglaw"]
 
 

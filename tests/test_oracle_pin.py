@@ -55,7 +55,7 @@ def assert_same(a, b, where):
 
 
 @pytest.mark.parametrize("name", ["tiny-sor", "tiny-bicg", "tiny-sorpc", "tiny-turbine",
-                                  "tiny-loglaw"])
+                                  "tiny-loglaw", "tiny-tgg"])
 def test_stage_by_stage_bit_identical(make_case, name):
     a, b = pair(make_case, name, tavg_start_time=0.0)
     assert a.max_diag() == b.max_diag()
