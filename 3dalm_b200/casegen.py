@@ -402,12 +402,14 @@ def main(argv=None):
     ap.add_argument("--max-it", type=int, help="eq.\"max iteration\"")
     ap.add_argument("--tol", type=float, help="eq.\"tolerance\"")
     ap.add_argument("--seed", type=int)
+    ap.add_argument("--dt", type=float, help="time step (default: the configuration's)")
     ap.add_argument("--no-state", action="store_true", help="skip the initial-state files")
     a = ap.parse_args(argv)
     over = {}
     if a.n:
         over["n"] = tuple(a.n)
-    for key, val in (("steps", a.steps), ("max_it", a.max_it), ("tol", a.tol), ("seed", a.seed)):
+    for key, val in (("steps", a.steps), ("max_it", a.max_it), ("tol", a.tol), ("seed", a.seed),
+                     ("dt", a.dt)):
         if val is not None:
             over[key] = val
     spec = config(a.config, **over)

@@ -85,9 +85,53 @@ __global__ void k_adj_alm_point(adj::AdjAlmPointArgs X) {
     if (a < X.A.ap_count) adj::adj_alm_point(X, a);
 }
 
-__global__ void k_adj_alm_scatter(adj::AdjAlmPointArgs X, Vec3<double> aU, double *grad) {
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        adj::adj_alm_scatter(X.A, X.ids, X.w, X.lU, X.gth, X.torque, X.weight, aU, grad);
+// adj::adj_alm_scatter in parallel without atomics: one thread per (point,
+// corner) entry e.  The entries are streamed through shared memory in
+// ascending order; the thread whose entry is the first one naming its cell
+// sums every entry of that cell in that order, starting from the cell's
+// value, and alone writes it: the serial loop's additions, in its order.
+// Block 0's first threads add the per-turbine gradients.
+constexpr int SCATTER_TILE = 256;
+
+__global__ void __launch_bounds__(SCATTER_TILE)
+k_adj_alm_scatter(adj::AdjAlmPointArgs X, Vec3<double> aU, double *grad) {
+    __shared__ long long sid[SCATTER_TILE];
+    __shared__ double sval[3][SCATTER_TILE];
+    const long long ne = 8 * (long long)X.A.ap_count;
+    if (blockIdx.x == 0)
+        for (int t = threadIdx.x; t < X.A.wt_count; t += SCATTER_TILE)
+            adj::adj_alm_turbine_grad(X.A, X.gth, X.torque, X.weight, t, grad);
+    const long long e = blockIdx.x * (long long)SCATTER_TILE + threadIdx.x;
+    const long long c = e < ne ? X.ids[e] : -1;
+    bool owner = c >= 0;
+    double acc[3] = {0, 0, 0};
+    for (long long t0 = 0; t0 < ne; t0 += SCATTER_TILE) {
+        const long long te = t0 + threadIdx.x;
+        __syncthreads();
+        if (te < ne) {
+            sid[threadIdx.x] = X.ids[te];
+            const double wq = X.w[te];
+            for (int m = 0; m < 3; m++) sval[m][threadIdx.x] = wq * X.lU[3 * (te / 8) + m];
+        } else {
+            sid[threadIdx.x] = -1;
+        }
+        __syncthreads();
+        if (!owner) continue;
+        const int nt = ne - t0 < SCATTER_TILE ? (int)(ne - t0) : SCATTER_TILE;
+        for (int u = 0; u < nt; u++) {
+            if (sid[u] != c) continue;
+            const long long eu = t0 + u;
+            if (eu < e) {  // an earlier entry owns the cell
+                owner = false;
+                break;
+            }
+            if (eu == e)
+                for (int m = 0; m < 3; m++) acc[m] = aU.c[m][c];
+            for (int m = 0; m < 3; m++) acc[m] += sval[m][u];
+        }
+    }
+    if (owner)
+        for (int m = 0; m < 3; m++) aU.c[m][c] = acc[m];
 }
 
 __global__ void k_adj_scale(double *v, long long n, double s) {
@@ -172,7 +216,9 @@ void launch_adj_alm(const LaunchCtx &L, const StepParams &P, const AlmDev &A,
     k_adj_alm_point<<<(A.ap_count + 63) / 64, 64, 0, L.s>>>(X);
     L.post(KK_ADJ_ALM);
     L.pre(KK_ADJ_ALM);
-    k_adj_alm_scatter<<<1, 32, 0, L.s>>>(X, aU, grad);
+    const long long ne = 8 * (long long)A.ap_count;
+    k_adj_alm_scatter<<<(int)((ne + SCATTER_TILE - 1) / SCATTER_TILE), SCATTER_TILE, 0, L.s>>>(X, aU,
+                                                                                            grad);
     L.post(KK_ADJ_ALM);
 }
 

@@ -766,25 +766,32 @@ DALM_HD void adj_alm_point(const AdjAlmPointArgs &X, int a) {
     X.torque[a] = e.torque.v;
 }
 
+// Turbine t's gradient (yaw deg, pitch deg, rotor speed): its points' terms
+// in blade-point order, then the explicit |Omega| factor of the power.
+DALM_HD void adj_alm_turbine_grad(const AlmDev &A, const double *gth, const double *torque,
+                                  double weight, int t, double *grad) {
+    double g[3] = {grad[3 * t], grad[3 * t + 1], grad[3 * t + 2]};
+    double tau = 0;
+    for (int a = t * A.ap_per_wt; a < (t + 1) * A.ap_per_wt; a++) {
+        tau += torque[a];
+        for (int p = 0; p < 3; p++) g[p] += gth[3 * (long long)a + p];
+    }
+    g[2] += weight * tau * sgn(A.wt[t].rot_speed);
+    for (int p = 0; p < 3; p++) grad[3 * t + p] = g[p];
+}
+
 // Serial, in blade-point order: the sampled-velocity adjoints onto the grid
-// and the per-turbine gradient (yaw deg, pitch deg, rotor speed), including
-// the explicit |Omega| factor of the power.
+// (entry e = 8 a + q adds w[e] lU[a] to cell ids[e]) and the per-turbine
+// gradient.  The device form (k_adj_alm_scatter) sums each cell's entries
+// in the same order and so gives the same bits.
 DALM_HD void adj_alm_scatter(const AlmDev &A, const long long *ids, const double *w,
                              const double *lU, const double *gth, const double *torque,
                              double weight, Vec3<double> aU, double *grad) {
-    for (int t = 0; t < A.wt_count; t++) {
-        double tau = 0;
-        for (int a = t * A.ap_per_wt; a < (t + 1) * A.ap_per_wt; a++) {
-            tau += torque[a];
-            for (int p = 0; p < 3; p++) grad[3 * t + p] += gth[3 * (long long)a + p];
-            for (int q = 0; q < 8; q++) {
-                long long c = ids[8 * (long long)a + q];
-                if (c < 0) continue;
-                double wq = w[8 * (long long)a + q];
-                for (int m = 0; m < 3; m++) aU.c[m][c] += wq * lU[3 * (long long)a + m];
-            }
-        }
-        grad[3 * t + 2] += weight * tau * sgn(A.wt[t].rot_speed);
+    for (int t = 0; t < A.wt_count; t++) adj_alm_turbine_grad(A, gth, torque, weight, t, grad);
+    for (long long e = 0; e < 8 * (long long)A.ap_count; e++) {
+        long long c = ids[e];
+        if (c < 0) continue;
+        for (int m = 0; m < 3; m++) aU.c[m][c] += w[e] * lU[3 * (e / 8) + m];
     }
 }
 

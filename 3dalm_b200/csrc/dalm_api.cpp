@@ -633,6 +633,11 @@ struct dalm_handle {
     // live in device memory); the fused kernels' ping-pong depends only on
     // the iteration's parity, and units start at even iterations.
     bool use_graphs() const { return opt.use_graphs && !opt.profile; }
+    // Iterations per graph unit: one for the multigrid inner solves, whose
+    // few (~90-kernel) iterations per pass are enqueued one at a time past
+    // the previous pass's count; GRAPH_UNIT for the Krylov solves.
+    bool mg_inner(int which) const { return which == 1 && mg_on; }
+    int unit_of(int which) const { return mg_inner(which) ? 1 : GRAPH_UNIT; }
     void enqueue_unit(int which, long long n0) {
         GraphUnit &gu = graph_unit[which];
         if (!gu.exec) {
@@ -640,7 +645,7 @@ struct dalm_handle {
             cudaGraph_t graph = nullptr;
             DALM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
             try {
-                for (int n = 0; n < GRAPH_UNIT; n++) enqueue_one(which, n0 + n, d_kst + which);
+                for (int n = 0; n < unit_of(which); n++) enqueue_one(which, n0 + n, d_kst + which);
             } catch (...) {
                 cudaStreamEndCapture(stream, &graph);
                 if (graph) cudaGraphDestroy(graph);
@@ -660,17 +665,19 @@ struct dalm_handle {
     long long run_batches(int which, long long hint, long long cap) {
         KrylovState *st = d_kst + which;
         long long issued = 0;
-        long long batch = opt.poisson_batch > 0
-                              ? opt.poisson_batch
-                              : std::min<long long>(256, hint > 12 ? hint / 2 : 4);
+        const bool mg = mg_inner(which);
+        long long batch = opt.poisson_batch > 0 ? opt.poisson_batch
+                          : mg                  ? std::max<long long>(1, hint)
+                                                : std::min<long long>(256, hint > 12 ? hint / 2 : 4);
         const bool graphs = use_graphs();
+        const int unit = unit_of(which);
         while (true) {
             batch = std::min<long long>(batch, std::max<long long>(1, cap - issued));
             if (graphs) {
                 // whole units; iterations past the stop return at once
-                const long long units = (batch + GRAPH_UNIT - 1) / GRAPH_UNIT;
-                for (long long u = 0; u < units; u++) enqueue_unit(which, issued + u * GRAPH_UNIT);
-                batch = units * GRAPH_UNIT;
+                const long long units = (batch + unit - 1) / unit;
+                for (long long u = 0; u < units; u++) enqueue_unit(which, issued + u * unit);
+                batch = units * unit;
             } else {
                 for (long long n = 0; n < batch; n++) enqueue_one(which, issued + n, st);
             }
@@ -683,6 +690,7 @@ struct dalm_handle {
             if (issued > cap + GRAPH_UNIT)
                 throw std::runtime_error("Poisson loop did not stop at its iteration limit");
             batch = opt.poisson_batch > 0 ? opt.poisson_batch
+                    : mg                  ? 1
                                           : std::max<long long>(8, std::min<long long>(96, issued / 8));
         }
         return h_kst[which].it;

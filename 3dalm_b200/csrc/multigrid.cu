@@ -15,120 +15,214 @@ namespace {
 
 constexpr int MG_THREADS = 256;
 
-// interior cells of a level, k fastest
-template <typename F>
-__device__ __forceinline__ void level_loop(const MgLevel &L, F f) {
-    const long long tot = L.cells();
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < tot;
-         n += (long long)gridDim.x * blockDim.x) {
-        int k = (int)(n % L.n[2]);
-        long long r = n / L.n[2];
-        int j = (int)(r % L.n[1]);
-        int i = (int)(r / L.n[1]);
-        f(i, j, k);
+// Interior cells of a level: one warp per (i, j) row, lane l taking
+// k = k0 + l + 32 u (u < U) for k0 = 0, 32 U, ... (coalesced rows; one
+// 32-bit division per row).  `load(i, j, k)` runs for all U cells before
+// `store(i, j, k, value)` runs for any, so every lane keeps U cells' loads
+// in flight: the compiler may not move a later cell's loads above an
+// earlier cell's stores, which it cannot prove do not alias them.
+template <int U, typename Ld, typename St>
+__device__ __forceinline__ void level_loop(const MgLevel &L, Ld load, St store) {
+    using T = decltype(load(0, 0, 0));
+    const int lane = threadIdx.x & 31;
+    const int nk = L.n[2];
+    const unsigned nj = (unsigned)L.n[1];
+    const unsigned rows = (unsigned)L.n[0] * nj;
+    const unsigned nw = gridDim.x * (blockDim.x >> 5);
+    for (unsigned row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < rows;
+         row += nw) {
+        const int i = (int)(row / nj), j = (int)(row - (unsigned)i * nj);
+        for (int k0 = 0; k0 < nk; k0 += 32 * U) {
+            T v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int k = k0 + lane + 32 * u;
+                if (k < nk) v[u] = load(i, j, k);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int k = k0 + lane + 32 * u;
+                if (k < nk) store(i, j, k, v[u]);
+            }
+        }
     }
 }
 
-// Zebra z-line half-sweep, one warp per column: lane l holds rows
-// k = l + 32 r (r < R, so the warp's loads and stores are coalesced rows)
-// and the tridiagonal system is solved by parallel cyclic reduction:
-// step delta combines every row with rows k -+ delta (through shuffles for
-// delta < 32, within the lane above) until each row stands alone; rows past
-// the column are identity rows.  The line operator is diagonally dominant,
-// which keeps the reduction stable without pivoting.  Same result as the
-// Thomas elimination of mg_thomas up to rounding (this file is compiled
-// with contraction and fast quotients).  Blocks only read columns
-// of the other colour and only write their own.
+// Zebra z-line half-sweep, one warp per column, by the partition method.
+// Lane l owns the R consecutive rows k = R l + s (s < R):
+//  1. the right-hand sides are formed in the coalesced layout k = l + 32 r
+//     and pass to the lanes' own rows through a per-warp shared-memory slab
+//     (slot k + k / 32: no bank conflicts either way for R = 1, 2, 4, 8);
+//  2. each lane eliminates its first R - 1 rows by a Thomas forward and back
+//     sweep into x_k = D_k - A_k y_{l-1} - C_k y_l, y_l being the value of
+//     its last row;
+//  3. the 32 last rows then form a tridiagonal system in the y_l alone,
+//     solved by parallel cyclic reduction over the lanes (5 shuffle steps);
+//  4. each lane expands its rows and the solution leaves through the slab in
+//     the coalesced layout.
+// Rows past the column are identity rows.  The line operator is diagonally
+// dominant, which keeps both eliminations stable without pivoting; the result
+// is mg_thomas's up to rounding (this file is compiled with contraction and
+// fast quotients).  Blocks only read columns of the other colour and only
+// write their own.
+//
+// With xc set, the half-sweep also applies the pending prolongation of the
+// coarse correction xc (level C): it reads each interior x or y neighbour
+// as x + xc(parent).  This is the first half-sweep after the coarse
+// correction; it overwrites its own colour, and the next half-sweep
+// overwrites the other colour from these values, so adding xc to the
+// neighbours it reads gives the prolongate-then-smooth result without the
+// separate pass over the level.
+struct ZlineArgs {
+    MgLevel L;
+    float *x;
+    const float *f;
+    int color, zero_start;
+    const float *xc;  // pending prolongation (or nullptr)
+    MgLevel C;
+};
+
 template <int R>
-__global__ void __launch_bounds__(MG_THREADS)
-k_mg_smooth(MgLevel L, float *x, const float *f, int color, int zero_start,
-            const KrylovState *st) {
+__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const KrylovState *st) {
+    __shared__ float slab[MG_THREADS / 32][33 * R];
     if (st->done) return;
+    const MgLevel &L = A.L;
+    float *__restrict__ x = A.x;
+    const float *__restrict__ f = A.f;
+    const float *__restrict__ xc = A.xc;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const long long ncol = (long long)L.n[0] * ((L.n[1] + 1) / 2);
-    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    float *sl = slab[threadIdx.x >> 5];
+    // column n of the colour: i = n / njh, j = 2 (n % njh) + (i + color) % 2
+    const unsigned njh = (unsigned)(L.n[1] + 1) / 2;
+    const unsigned ncol = (unsigned)L.n[0] * njh;
+    const unsigned nw = gridDim.x * (blockDim.x >> 5);
     const int nk = L.n[2];
-    const bool zero = zero_start != 0;
-    for (long long col = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5);
-         col < ncol; col += nw) {
-        int i, j;
-        if (!mg_color_column(L, col, color, i, j)) continue;  // uniform in the warp
+    const bool zero = A.zero_start != 0;
+    const int kshift = A.C.fac[2] == 2 ? 1 : 0;
+    for (unsigned col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); col < ncol;
+         col += nw) {
+        const int i = (int)(col / njh);
+        const int j = 2 * (int)(col - (unsigned)i * njh) + ((i + A.color) & 1);
+        if (j >= L.n[1]) continue;  // uniform in the warp
+        const long long c0 = L.at(i, j, 0);
+        // parents of the interior x and y neighbours (-1: boundary, no correction)
+        long long pe = -1, pw = -1, pn = -1, ps = -1;
+        if (xc) {
+            const MgLevel &C = A.C;
+            const int I = i / C.fac[0], J = j / C.fac[1];
+            if (i + 1 < L.n[0]) pe = C.at((i + 1) / C.fac[0], J, 0);
+            if (i > 0) pw = C.at((i - 1) / C.fac[0], J, 0);
+            if (j + 1 < L.n[1]) pn = C.at(I, (j + 1) / C.fac[1], 0);
+            if (j > 0) ps = C.at(I, (j - 1) / C.fac[1], 0);
+        }
+        // the column's constants (mg_zline_coef and mg_zline_rhs per row)
+        const float wi = L.w[0][i], wj = L.w[1][j];
+        const float xe = L.cf[0][i + 1], xw = L.cf[0][i], yn = L.cf[1][j + 1], ys = L.cf[1][j];
+        const float az = wi * wj, sxy = wj * (xe + xw) + wi * (yn + ys);
+        const float *w2 = L.w[2], *cf2 = L.cf[2];
+        // all of the column's loads first, then the slab
+        float rhs[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int k = lane + 32 * r;
+            rhs[r] = 0.f;
+            if (k < nk) {
+                const long long q = c0 + k;
+                rhs[r] = f[q];
+                if (!zero) {
+                    float ve = x[q + L.g.sx], vw = x[q - L.g.sx], vn = x[q + L.g.sy],
+                          vs = x[q - L.g.sy];
+                    if (xc) {
+                        const int K = k >> kshift;
+                        if (pe >= 0) ve += xc[pe + K];
+                        if (pw >= 0) vw += xc[pw + K];
+                        if (pn >= 0) vn += xc[pn + K];
+                        if (ps >= 0) vs += xc[ps + K];
+                    }
+                    rhs[r] += w2[k] * (wj * (xe * ve + xw * vw) + wi * (yn * vn + ys * vs));
+                }
+            }
+        }
+        __syncwarp();  // the previous column's reads of the slab are done
+#pragma unroll
+        for (int r = 0; r < R; r++) sl[lane + 33 * r] = rhs[r];
+        __syncwarp();
         float a[R], b[R], c[R], d[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int k = lane + 32 * r;
+        for (int s = 0; s < R; s++) {
+            const int k = R * lane + s;
+            d[s] = sl[k + (k >> 5)];
             if (k < nk) {
-                float lo, hi, bb;
-                mg_zline_coef(L, i, j, k, lo, hi, bb);
-                a[r] = -lo;
-                c[r] = -hi;
-                b[r] = bb;
-                d[r] = mg_zline_rhs(L, x, f, i, j, k, zero);
+                const float lo = az * cf2[k], hi = az * cf2[k + 1];
+                a[s] = -lo;
+                b[s] = w2[k] * sxy + lo + hi;
+                c[s] = -hi;
             } else {
-                a[r] = 0.f;
-                c[r] = 0.f;
-                b[r] = 1.f;
-                d[r] = 0.f;
+                a[s] = 0.f;
+                b[s] = 1.f;
+                c[s] = 0.f;
             }
         }
+        // 2. rows s < R - 1: x_s = D_s - A_s y_{l-1} - C_s y_l (in e, fa, g)
+        float e[R], fa[R], g[R];
+        float ra = a[R - 1], rb = b[R - 1], rc = c[R - 1], rd = d[R - 1];
+        if (R > 1) {
 #pragma unroll
-        for (int delta = 1; delta < 32 * R; delta <<= 1) {
-            float na[R], nb[R], nc[R], nd[R];
-#pragma unroll
-            for (int r = 0; r < R; r++) {
-                // row k - delta and row k + delta (identity outside the column)
-                float am = 0.f, bm = 1.f, cm = 0.f, dm = 0.f, ap = 0.f, bp = 1.f, cp = 0.f, dp = 0.f;
-                if (delta < 32) {
-                    const int src_m = (lane - delta) & 31, src_p = (lane + delta) & 31;
-                    const bool wrap_m = lane < delta, wrap_p = lane + delta >= 32;
-                    // same register r, or r - 1 / r + 1 across the lane wrap
-                    const float a0 = __shfl_sync(full, a[r], src_m), b0 = __shfl_sync(full, b[r], src_m);
-                    const float c0 = __shfl_sync(full, c[r], src_m), d0 = __shfl_sync(full, d[r], src_m);
-                    const float a1 = __shfl_sync(full, r > 0 ? a[r > 0 ? r - 1 : 0] : 0.f, src_m);
-                    const float b1 = __shfl_sync(full, r > 0 ? b[r > 0 ? r - 1 : 0] : 1.f, src_m);
-                    const float c1 = __shfl_sync(full, r > 0 ? c[r > 0 ? r - 1 : 0] : 0.f, src_m);
-                    const float d1 = __shfl_sync(full, r > 0 ? d[r > 0 ? r - 1 : 0] : 0.f, src_m);
-                    am = wrap_m ? a1 : a0; bm = wrap_m ? b1 : b0; cm = wrap_m ? c1 : c0; dm = wrap_m ? d1 : d0;
-                    const float a2 = __shfl_sync(full, a[r], src_p), b2 = __shfl_sync(full, b[r], src_p);
-                    const float c2 = __shfl_sync(full, c[r], src_p), d2 = __shfl_sync(full, d[r], src_p);
-                    const float a3 = __shfl_sync(full, r + 1 < R ? a[r + 1 < R ? r + 1 : r] : 0.f, src_p);
-                    const float b3 = __shfl_sync(full, r + 1 < R ? b[r + 1 < R ? r + 1 : r] : 1.f, src_p);
-                    const float c3 = __shfl_sync(full, r + 1 < R ? c[r + 1 < R ? r + 1 : r] : 0.f, src_p);
-                    const float d3 = __shfl_sync(full, r + 1 < R ? d[r + 1 < R ? r + 1 : r] : 0.f, src_p);
-                    ap = wrap_p ? a3 : a2; bp = wrap_p ? b3 : b2; cp = wrap_p ? c3 : c2; dp = wrap_p ? d3 : d2;
-                } else {
-                    const int m = delta / 32;
-                    if (r - m >= 0) {
-                        am = a[r - m >= 0 ? r - m : 0]; bm = b[r - m >= 0 ? r - m : 0];
-                        cm = c[r - m >= 0 ? r - m : 0]; dm = d[r - m >= 0 ? r - m : 0];
-                    }
-                    if (r + m < R) {
-                        ap = a[r + m < R ? r + m : 0]; bp = b[r + m < R ? r + m : 0];
-                        cp = c[r + m < R ? r + m : 0]; dp = d[r + m < R ? r + m : 0];
-                    }
-                }
-                // approximate quotients (2 ulp): the preconditioner needs no
-                // correctly rounded division
-                const float al = -__fdividef(a[r], bm), ga = -__fdividef(c[r], bp);
-                na[r] = al * am;
-                nc[r] = ga * cp;
-                nb[r] = b[r] + al * cm + ga * ap;
-                nd[r] = d[r] + al * dm + ga * dp;
+            for (int s = 0; s < R - 1; s++) {
+                const float den = s == 0 ? b[0] : b[s] - a[s] * g[s > 0 ? s - 1 : 0];
+                const float q = __fdividef(1.f, den);
+                e[s] = (s == 0 ? d[0] : d[s] - a[s] * e[s > 0 ? s - 1 : 0]) * q;
+                fa[s] = (s == 0 ? a[0] : -a[s] * fa[s > 0 ? s - 1 : 0]) * q;
+                g[s] = c[s] * q;
             }
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                a[r] = na[r];
-                b[r] = nb[r];
-                c[r] = nc[r];
-                d[r] = nd[r];
+            for (int s = R - 3; s >= 0; s--) {
+                e[s] -= g[s] * e[s + 1];
+                fa[s] -= g[s] * fa[s + 1];
+                g[s] = -g[s] * g[s + 1];
             }
+            // 3. the last row, with x of the next lane's first row
+            float An = __shfl_down_sync(full, fa[0], 1), Cn = __shfl_down_sync(full, g[0], 1);
+            float Dn = __shfl_down_sync(full, e[0], 1);
+            if (lane == 31) An = Cn = Dn = 0.f;
+            const float al = a[R - 1], cl = c[R - 1];
+            ra = -al * fa[R - 2];
+            rb = b[R - 1] - al * g[R - 2] - cl * An;
+            rc = -cl * Cn;
+            rd = d[R - 1] - al * e[R - 2] - cl * Dn;
         }
-        const long long c0 = L.at(i, j, 0);
+#pragma unroll
+        for (int delta = 1; delta < 32; delta <<= 1) {
+            float am = __shfl_up_sync(full, ra, delta), bm = __shfl_up_sync(full, rb, delta);
+            float cm = __shfl_up_sync(full, rc, delta), dm = __shfl_up_sync(full, rd, delta);
+            float ap = __shfl_down_sync(full, ra, delta), bp = __shfl_down_sync(full, rb, delta);
+            float cp = __shfl_down_sync(full, rc, delta), dp = __shfl_down_sync(full, rd, delta);
+            if (lane < delta) am = 0.f, bm = 1.f, cm = 0.f, dm = 0.f;  // identity rows
+            if (lane + delta >= 32) ap = 0.f, bp = 1.f, cp = 0.f, dp = 0.f;
+            // approximate quotients (2 ulp): the preconditioner needs no
+            // correctly rounded division
+            const float alpha = -__fdividef(ra, bm), gamma = -__fdividef(rc, bp);
+            rb += alpha * cm + gamma * ap;
+            rd += alpha * dm + gamma * dp;
+            ra = alpha * am;
+            rc = gamma * cp;
+        }
+        const float y = __fdividef(rd, rb);
+        float ym = __shfl_up_sync(full, y, 1);
+        if (lane == 0) ym = 0.f;
+        // 4. expand and store through the slab
+#pragma unroll
+        for (int s = 0; s < R; s++) {
+            const int k = R * lane + s;
+            sl[k + (k >> 5)] = s == R - 1 ? y : e[s < R - 1 ? s : 0] - fa[s < R - 1 ? s : 0] * ym -
+                                                    g[s < R - 1 ? s : 0] * y;
+        }
+        __syncwarp();
 #pragma unroll
         for (int r = 0; r < R; r++) {
             const int k = lane + 32 * r;
-            if (k < nk) x[c0 + k] = __fdividef(d[r], b[r]);
+            if (k < nk) x[c0 + k] = sl[k + r];
         }
     }
 }
@@ -137,40 +231,35 @@ k_mg_smooth(MgLevel L, float *x, const float *f, int color, int zero_start,
 constexpr int ZL_MAX_R = 8;
 
 template <int R>
-void zline_launch(const LaunchCtx &L, const MgLevel &v, float *x, const float *f, int color,
-                  int zero, const KrylovState *st, int blocks) {
-    k_mg_smooth<R><<<blocks, MG_THREADS, 0, L.s>>>(v, x, f, color, zero, st);
+void zline_launch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st, int blocks) {
+    k_mg_smooth<R><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
 }
 
-void zline_dispatch(const LaunchCtx &L, const MgLevel &v, float *x, const float *f, int color,
-                    int zero, const KrylovState *st) {
+void zline_dispatch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st) {
+    const MgLevel &v = a.L;
     const long long ncol = (long long)v.n[0] * ((v.n[1] + 1) / 2);
     long long nb = (ncol + MG_THREADS / 32 - 1) / (MG_THREADS / 32);
     if (nb > L.blocks) nb = L.blocks;
     const int R = (v.n[2] + 31) / 32;
     switch (R) {
-    case 1: zline_launch<1>(L, v, x, f, color, zero, st, (int)nb); break;
-    case 2: zline_launch<2>(L, v, x, f, color, zero, st, (int)nb); break;
-    case 3: zline_launch<3>(L, v, x, f, color, zero, st, (int)nb); break;
-    case 4: zline_launch<4>(L, v, x, f, color, zero, st, (int)nb); break;
-    case 5: zline_launch<5>(L, v, x, f, color, zero, st, (int)nb); break;
-    case 6: zline_launch<6>(L, v, x, f, color, zero, st, (int)nb); break;
-    case 7: zline_launch<7>(L, v, x, f, color, zero, st, (int)nb); break;
-    default: zline_launch<8>(L, v, x, f, color, zero, st, (int)nb); break;
+    case 1: zline_launch<1>(L, a, st, (int)nb); break;
+    case 2: zline_launch<2>(L, a, st, (int)nb); break;
+    case 3: zline_launch<3>(L, a, st, (int)nb); break;
+    case 4: zline_launch<4>(L, a, st, (int)nb); break;
+    case 5: zline_launch<5>(L, a, st, (int)nb); break;
+    case 6: zline_launch<6>(L, a, st, (int)nb); break;
+    case 7: zline_launch<7>(L, a, st, (int)nb); break;
+    default: zline_launch<8>(L, a, st, (int)nb); break;
     }
 }
 
 __global__ void __launch_bounds__(MG_THREADS)
-k_mg_restrict(MgLevel F, MgLevel C, const float *x, const float *f, float *fc,
+k_mg_restrict(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, int skip,
               const KrylovState *st) {
     if (st->done) return;
-    level_loop(C, [&](int I, int J, int K) { mg_restrict_cell(F, C, x, f, fc, I, J, K); });
-}
-
-__global__ void __launch_bounds__(MG_THREADS)
-k_mg_prolong(MgLevel F, MgLevel C, float *x, const float *xc, const KrylovState *st) {
-    if (st->done) return;
-    level_loop(F, [&](int i, int j, int k) { mg_prolong_cell(F, C, x, xc, i, j, k); });
+    level_loop<2>(
+        C, [&](int I, int J, int K) { return mg_restrict_sum(F, C, x, f, I, J, K, skip); },
+        [&](int I, int J, int K, float s) { fc[C.at(I, J, K)] = s; });
 }
 
 // x = K^-1 f on the coarsest level: one warp per row of the dense inverse
@@ -198,11 +287,13 @@ __device__ __forceinline__ float cell_volume(const MgLevel &L, int i, int j, int
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_rhs(MgLevel L, float *r, float *e, float md, const KrylovState *st) {
     if (st->done) return;
-    level_loop(L, [&](int i, int j, int k) {
-        const long long c = L.at(i, j, k);
-        r[c] = -md * cell_volume(L, i, j, k) * r[c];
-        e[c] = 0.f;
-    });
+    level_loop<4>(
+        L, [&](int i, int j, int k) { return r[L.at(i, j, k)]; },
+        [&](int i, int j, int k, float rv) {
+            const long long c = L.at(i, j, k);
+            r[c] = -md * cell_volume(L, i, j, k) * rv;
+            e[c] = 0.f;
+        });
 }
 
 __device__ __forceinline__ void breakdown(KrylovState *st) {
@@ -216,11 +307,16 @@ k_mg_first(MgLevel L, const float *r, const float *z, float *p, Partials<1> part
            KrylovState *st) {
     if (st->done) return;
     double acc = 0;
-    level_loop(L, [&](int i, int j, int k) {
-        const long long c = L.at(i, j, k);
-        p[c] = z[c];
-        acc += (double)r[c] * (double)z[c];
-    });
+    level_loop<4>(
+        L,
+        [&](int i, int j, int k) {
+            const long long c = L.at(i, j, k);
+            return make_float2(r[c], z[c]);
+        },
+        [&](int i, int j, int k, float2 v) {
+            p[L.at(i, j, k)] = v.y;
+            acc += (double)v.x * (double)v.y;
+        });
     double v[1] = {acc};
     if (grid_reduce<1>(v, 0u, part) && threadIdx.x == 0) {
         st->rho = v[0];
@@ -234,12 +330,15 @@ __global__ void __launch_bounds__(MG_THREADS)
 k_mg_spmv(MgLevel L, const float *p, float *q, Partials<1> part, KrylovState *st) {
     if (st->done) return;
     double acc = 0;
-    level_loop(L, [&](int i, int j, int k) {
-        const long long c = L.at(i, j, k);
-        const float v = mg_apply(L, p, i, j, k);
-        q[c] = v;
-        acc += (double)p[c] * (double)v;
-    });
+    level_loop<2>(
+        L,
+        [&](int i, int j, int k) {
+            return make_float2(mg_apply(L, p, i, j, k), p[L.at(i, j, k)]);
+        },
+        [&](int i, int j, int k, float2 v) {
+            q[L.at(i, j, k)] = v.x;
+            acc += (double)v.y * (double)v.x;
+        });
     double v[1] = {acc};
     if (grid_reduce<1>(v, 0u, part) && threadIdx.x == 0) {
         if (!(v[0] > 0.0) || !isfinite(v[0])) breakdown(st);
@@ -254,14 +353,20 @@ k_mg_update(MgLevel L, float *e, float *r, const float *p, const float *q, float
     if (st->done) return;
     const float a = (float)st->alpha;
     double acc = 0;
-    level_loop(L, [&](int i, int j, int k) {
-        const long long c = L.at(i, j, k);
-        e[c] += a * p[c];
-        const float rn = r[c] - a * q[c];
-        r[c] = rn;
-        const double ra = (double)rn / ((double)md * (double)cell_volume(L, i, j, k));
-        acc += ra * ra;
-    });
+    level_loop<4>(
+        L,
+        [&](int i, int j, int k) {
+            const long long c = L.at(i, j, k);
+            return make_float4(e[c], p[c], r[c], q[c]);
+        },
+        [&](int i, int j, int k, float4 v) {
+            const long long c = L.at(i, j, k);
+            e[c] = v.x + a * v.y;
+            const float rn = v.z - a * v.w;
+            r[c] = rn;
+            const double ra = (double)rn / ((double)md * (double)cell_volume(L, i, j, k));
+            acc += ra * ra;
+        });
     double v[1] = {acc};
     if (grid_reduce<1>(v, 0u, part) && threadIdx.x == 0) {
         st->err = sqrt(v[0] / st->ncell);
@@ -276,10 +381,13 @@ __global__ void __launch_bounds__(MG_THREADS)
 k_mg_rz(MgLevel L, const float *r, const float *z, Partials<1> part, KrylovState *st) {
     if (st->done) return;
     double acc = 0;
-    level_loop(L, [&](int i, int j, int k) {
-        const long long c = L.at(i, j, k);
-        acc += (double)r[c] * (double)z[c];
-    });
+    level_loop<4>(
+        L,
+        [&](int i, int j, int k) {
+            const long long c = L.at(i, j, k);
+            return make_float2(r[c], z[c]);
+        },
+        [&](int, int, int, float2 v) { acc += (double)v.x * (double)v.y; });
     double v[1] = {acc};
     if (grid_reduce<1>(v, 0u, part) && threadIdx.x == 0) {
         if (!isfinite(v[0])) {
@@ -296,10 +404,13 @@ __global__ void __launch_bounds__(MG_THREADS)
 k_mg_pupdate(MgLevel L, const float *z, float *p, const KrylovState *st) {
     if (st->done) return;
     const float b = (float)st->beta;
-    level_loop(L, [&](int i, int j, int k) {
-        const long long c = L.at(i, j, k);
-        p[c] = z[c] + b * p[c];
-    });
+    level_loop<4>(
+        L,
+        [&](int i, int j, int k) {
+            const long long c = L.at(i, j, k);
+            return make_float2(z[c], p[c]);
+        },
+        [&](int i, int j, int k, float2 v) { p[L.at(i, j, k)] = v.x + b * v.y; });
 }
 
 int blocks_for(long long n, int cap) {
@@ -309,19 +420,34 @@ int blocks_for(long long n, int cap) {
 }
 
 // launches the V-cycle's steps (mg_vcycle's executor)
+// The V-cycle's steps (mg_vcycle's executor).  Two steps are folded into
+// the smoothing: the restriction sums only the children of the colour
+// smoothed before the last half-sweep (the last half-sweep leaves its own
+// colour's residual at zero: each of its lines is solved exactly with
+// neighbours it did not change), and each prolongation is applied by the
+// next half-sweep (ZlineArgs::xc) instead of a pass of its own.
 struct DeviceCycle {
     const LaunchCtx &L;
     const MgDev &M;
     const KrylovState *st;
+    int last_color[MG_MAX_LEVELS];
+    bool pending[MG_MAX_LEVELS] = {};
     void smooth(int l, int color, bool zero) {
+        ZlineArgs a{M.L[l], M.x[l], M.f[l], color, zero ? 1 : 0, nullptr, M.L[l]};
+        if (pending[l]) {
+            a.xc = M.x[l + 1];
+            a.C = M.L[l + 1];
+            pending[l] = false;
+        }
         L.pre(KK_MG_SMOOTH);
-        zline_dispatch(L, M.L[l], M.x[l], M.f[l], color, zero ? 1 : 0, st);
+        zline_dispatch(L, a, st);
         L.post(KK_MG_SMOOTH);
+        last_color[l] = color;
     }
     void restrict(int l) {
         L.pre(KK_MG_TRANSFER);
         k_mg_restrict<<<blocks_for(M.L[l + 1].cells(), L.blocks), MG_THREADS, 0, L.s>>>(
-            M.L[l], M.L[l + 1], M.x[l], M.f[l], M.f[l + 1], st);
+            M.L[l], M.L[l + 1], M.x[l], M.f[l], M.f[l + 1], last_color[l], st);
         L.post(KK_MG_TRANSFER);
     }
     void coarse() {
@@ -331,13 +457,9 @@ struct DeviceCycle {
             M.L[l], M.kinv, M.ncoarse, M.f[l], M.x[l], st);
         L.post(KK_MG_COARSE);
     }
-    void prolong(int l) {
-        L.pre(KK_MG_TRANSFER);
-        k_mg_prolong<<<blocks_for(M.L[l].cells(), L.blocks), MG_THREADS, 0, L.s>>>(
-            M.L[l], M.L[l + 1], M.x[l], M.x[l + 1], st);
-        L.post(KK_MG_TRANSFER);
-    }
+    void prolong(int l) { pending[l] = true; }
 };
+static_assert(MG_NU >= 1, "the prolongation is applied by the first smoothing after it");
 
 }  // namespace
 

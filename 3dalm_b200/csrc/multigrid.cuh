@@ -142,17 +142,27 @@ DALM_HD bool mg_color_column(const MgLevel &L, long long n, int color, int &i, i
     return j < L.n[1];
 }
 
-// coarse cell (I,J,K): the sum of its children's residuals f - K x
-DALM_HD void mg_restrict_cell(const MgLevel &F, const MgLevel &C, const float *x, const float *f,
-                              float *fc, int I, int J, int K) {
+// coarse cell (I,J,K): the sum of its children's residuals f - K x, leaving
+// out the children of colour `skip` ((i + j) % 2; -1: none), whose residual
+// the caller knows to be zero
+DALM_HD float mg_restrict_sum(const MgLevel &F, const MgLevel &C, const float *x, const float *f,
+                              int I, int J, int K, int skip = -1) {
     float s = 0;
     for (int a = 0; a < C.fac[0]; a++)
-        for (int b = 0; b < C.fac[1]; b++)
+        for (int b = 0; b < C.fac[1]; b++) {
+            const int i = I * C.fac[0] + a, j = J * C.fac[1] + b;
+            if (((i + j) & 1) == skip) continue;
             for (int c = 0; c < C.fac[2]; c++) {
-                const int i = I * C.fac[0] + a, j = J * C.fac[1] + b, k = K * C.fac[2] + c;
+                const int k = K * C.fac[2] + c;
                 s += f[F.at(i, j, k)] - mg_apply(F, x, i, j, k);
             }
-    fc[C.at(I, J, K)] = s;
+        }
+    return s;
+}
+
+DALM_HD void mg_restrict_cell(const MgLevel &F, const MgLevel &C, const float *x, const float *f,
+                              float *fc, int I, int J, int K) {
+    fc[C.at(I, J, K)] = mg_restrict_sum(F, C, x, f, I, J, K);
 }
 
 // fine cell (i,j,k) += its parent's correction
