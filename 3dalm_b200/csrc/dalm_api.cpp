@@ -107,6 +107,7 @@ struct dalm_handle {
     bool mg_on = false;
     MgDev mgd;
     MgPcgBufs mgb{};
+    MixedGeom geo{};  // the FP32 predictor's mesh table
     FusedBufs fb{};
     bool fused = false;  // BiCGStab iterations as fused half-iteration kernels
     PoissonConfig pcfg{};
@@ -287,6 +288,18 @@ struct dalm_handle {
         mesh.x = upload(cs.x); mesh.y = upload(cs.y); mesh.z = upload(cs.z);
         mesh.dx = upload(cs.dx); mesh.dy = upload(cs.dy); mesh.dz = upload(cs.dz);
         build_coefficients();
+        {
+            const std::vector<double> *ctr[3] = {&cs.x, &cs.y, &cs.z}, *wid[3] = {&cs.dx, &cs.dy, &cs.dz};
+            for (int a = 0; a < 3; a++) {
+                const std::vector<double> &x = *ctr[a], &d = *wid[a];
+                std::vector<float4> t(x.size(), make_float4(0.f, 0.f, 0.f, 0.f));
+                for (size_t n = 1; n + 1 < x.size(); n++)
+                    t[n] = make_float4((float)(1.0 / d[n]), (float)(1.0 / (x[n + 1] - x[n])),
+                                       (float)(1.0 / (x[n] - x[n - 1])),
+                                       (float)(1.0 / (x[n + 1] - x[n - 1])));
+                geo.ax[a] = upload(t);
+            }
+        }
 
         size_t n = (size_t)g.total;
         for (int b = 0; b < 2; b++)
@@ -585,7 +598,7 @@ struct dalm_handle {
         StageTimer t(this, DALM_STAGE_PREDICT);
         P.fbox = fbox;
         if (mixed)
-            launch_predict_f32(L, P, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
+            launch_predict_f32(L, P, geo, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
         else
             launch_predict(L, P, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
         ucur = 1 - ucur;  // the old buffer is now Uold

@@ -93,8 +93,14 @@ __device__ inline void warp_serial_sums(const Grid &g, Term term, double (&total
 void launch_predict(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,
                     Vec3<double> unew, Vec3<const double> ju, Vec3<const double> f);
 // the mixed-precision form's predictor: the increment in FP32 (flow_mixed.cu)
-void launch_predict_f32(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,
-                        Vec3<double> unew, Vec3<const double> ju, Vec3<const double> f);
+// with the mesh as one FP32 table per axis: for stored index n,
+// {1/d_n, 1/(x_{n+1} - x_n), 1/(x_n - x_{n-1}), 1/(x_{n+1} - x_{n-1})}
+struct MixedGeom {
+    const float4 *ax[3];
+};
+void launch_predict_f32(const LaunchCtx &L, const StepParams &P, const MixedGeom &geo,
+                        Vec3<const double> uold, Vec3<double> unew, Vec3<const double> ju,
+                        Vec3<const double> f);
 void launch_flux_rhs(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                      Vec3<double> ju, double *b);
 void launch_flux_only(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,

@@ -17,13 +17,15 @@ constexpr int MG_THREADS = 256;
 
 // Interior cells of a level: one warp per (i, j) row, lane l taking
 // k = k0 + l + 32 u (u < U) for k0 = 0, 32 U, ... (coalesced rows; one
-// 32-bit division per row).  `load(i, j, k)` runs for all U cells before
-// `store(i, j, k, value)` runs for any, so every lane keeps U cells' loads
-// in flight: the compiler may not move a later cell's loads above an
-// earlier cell's stores, which it cannot prove do not alias them.
-template <int U, typename Ld, typename St>
-__device__ __forceinline__ void level_loop(const MgLevel &L, Ld load, St store) {
-    using T = decltype(load(0, 0, 0));
+// 32-bit division per row).  `prep(i, j)` makes the row's constants once;
+// `load(row, k)` runs for all U cells before `store(row, k, value)` runs for
+// any, so every lane keeps U cells' loads in flight: the compiler may not
+// move a later cell's loads above an earlier cell's stores, which it cannot
+// prove do not alias them.
+template <int U, typename Prep, typename Ld, typename St>
+__device__ __forceinline__ void level_loop(const MgLevel &L, Prep prep, Ld load, St store) {
+    using Row = decltype(prep(0, 0));
+    using T = decltype(load(prep(0, 0), 0));
     const int lane = threadIdx.x & 31;
     const int nk = L.n[2];
     const unsigned nj = (unsigned)L.n[1];
@@ -32,20 +34,61 @@ __device__ __forceinline__ void level_loop(const MgLevel &L, Ld load, St store) 
     for (unsigned row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < rows;
          row += nw) {
         const int i = (int)(row / nj), j = (int)(row - (unsigned)i * nj);
+        const Row R = prep(i, j);
         for (int k0 = 0; k0 < nk; k0 += 32 * U) {
             T v[U];
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int k = k0 + lane + 32 * u;
-                if (k < nk) v[u] = load(i, j, k);
+                if (k < nk) v[u] = load(R, k);
             }
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int k = k0 + lane + 32 * u;
-                if (k < nk) store(i, j, k, v[u]);
+                if (k < nk) store(R, k, v[u]);
             }
         }
     }
+}
+
+// Row (i, j) of a level with its constants: (K x) at k is mg_apply with the
+// row's factors taken out of the per-cell sums.
+struct MgRow {
+    long long c0;
+    int sx, sy;
+    float w0, w1, az, xe, xw, yn, ys, sxy;
+    MgRow() = default;
+    __device__ __forceinline__ MgRow(const MgLevel &L, int i, int j) {
+        c0 = L.at(i, j, 0);
+        sx = (int)L.g.sx;
+        sy = (int)L.g.sy;
+        w0 = L.w[0][i];
+        w1 = L.w[1][j];
+        az = w0 * w1;
+        xe = L.cf[0][i + 1];
+        xw = L.cf[0][i];
+        yn = L.cf[1][j + 1];
+        ys = L.cf[1][j];
+        sxy = w1 * (xe + xw) + w0 * (yn + ys);
+    }
+    __device__ __forceinline__ float apply(const MgLevel &L, const float *x, int k) const {
+        const float *xr = x + c0 + k;
+        const float w2 = L.w[2][k], zt = L.cf[2][k + 1], zb = L.cf[2][k];
+        const float diag = w2 * sxy + az * (zt + zb);
+        const float nb =
+            w2 * (w1 * (xe * xr[sx] + xw * xr[-sx]) + w0 * (yn * xr[sy] + ys * xr[-sy])) +
+            az * (zt * xr[1] + zb * xr[-1]);
+        return diag * xr[0] - nb;
+    }
+};
+
+// a row's storage offset and area factor w0 w1 (cell volume = w01 w2[k])
+struct MgRowBase {
+    long long c0;
+    float w01;
+};
+__device__ __forceinline__ MgRowBase row_base(const MgLevel &L, int i, int j) {
+    return MgRowBase{L.at(i, j, 0), L.w[0][i] * L.w[1][j]};
 }
 
 // Zebra z-line half-sweep, one warp per column, by the partition method.
@@ -121,6 +164,9 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const Kry
         const float xe = L.cf[0][i + 1], xw = L.cf[0][i], yn = L.cf[1][j + 1], ys = L.cf[1][j];
         const float az = wi * wj, sxy = wj * (xe + xw) + wi * (yn + ys);
         const float *w2 = L.w[2], *cf2 = L.cf[2];
+        // the column and its x and y neighbours, from k = 0
+        const float *fr = f + c0, *xre = x + c0 + L.g.sx, *xrw = x + c0 - L.g.sx,
+                    *xrn = x + c0 + L.g.sy, *xrs = x + c0 - L.g.sy;
         // all of the column's loads first, then the slab
         float rhs[R];
 #pragma unroll
@@ -128,11 +174,9 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const Kry
             const int k = lane + 32 * r;
             rhs[r] = 0.f;
             if (k < nk) {
-                const long long q = c0 + k;
-                rhs[r] = f[q];
+                rhs[r] = fr[k];
                 if (!zero) {
-                    float ve = x[q + L.g.sx], vw = x[q - L.g.sx], vn = x[q + L.g.sy],
-                          vs = x[q - L.g.sy];
+                    float ve = xre[k], vw = xrw[k], vn = xrn[k], vs = xrs[k];
                     if (xc) {
                         const int K = k >> kshift;
                         if (pe >= 0) ve += xc[pe + K];
@@ -253,13 +297,51 @@ void zline_dispatch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *s
     }
 }
 
+// coarse cell (I,J,K) = the sum of its children's residuals f - K x,
+// leaving out the children of colour `skip` (as mg_restrict_sum).  One warp
+// per coarse row, U coarse cells per lane at a time: the child rows (at most
+// 2 x 2, levels merge at most two cells per axis) are visited one after the
+// other, each with its row constants, and the sums are stored at the end.
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_restrict(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, int skip,
               const KrylovState *st) {
     if (st->done) return;
-    level_loop<2>(
-        C, [&](int I, int J, int K) { return mg_restrict_sum(F, C, x, f, I, J, K, skip); },
-        [&](int I, int J, int K, float s) { fc[C.at(I, J, K)] = s; });
+    constexpr int U = 4;
+    const int lane = threadIdx.x & 31;
+    const int nk = C.n[2], f2 = C.fac[2];
+    const unsigned nj = (unsigned)C.n[1];
+    const unsigned rows = (unsigned)C.n[0] * nj;
+    const unsigned nw = gridDim.x * (blockDim.x >> 5);
+    for (unsigned row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < rows;
+         row += nw) {
+        const int I = (int)(row / nj), J = (int)(row - (unsigned)I * nj);
+        const long long cc = C.at(I, J, 0);
+        for (int k0 = 0; k0 < nk; k0 += 32 * U) {
+            float s[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) s[u] = 0.f;
+            for (int a = 0; a < C.fac[0]; a++)
+                for (int b = 0; b < C.fac[1]; b++) {
+                    const int i = I * C.fac[0] + a, j = J * C.fac[1] + b;
+                    if (((i + j) & 1) == skip) continue;
+                    const MgRow R(F, i, j);
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        const int K = k0 + lane + 32 * u;
+                        if (K < nk)
+                            for (int c = 0; c < f2; c++) {
+                                const int k = K * f2 + c;
+                                s[u] += f[R.c0 + k] - R.apply(F, x, k);
+                            }
+                    }
+                }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int K = k0 + lane + 32 * u;
+                if (K < nk) fc[cc + K] = s[u];
+            }
+        }
+    }
 }
 
 // x = K^-1 f on the coarsest level: one warp per row of the dense inverse
@@ -279,20 +361,16 @@ k_mg_coarse(MgLevel C, const float *kinv, int n, const float *f, float *x,
     }
 }
 
-__device__ __forceinline__ float cell_volume(const MgLevel &L, int i, int j, int k) {
-    return L.w[0][i] * L.w[1][j] * L.w[2][k];
-}
-
 // f = -max_diag vol r (in place), e = 0
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_rhs(MgLevel L, float *r, float *e, float md, const KrylovState *st) {
     if (st->done) return;
     level_loop<4>(
-        L, [&](int i, int j, int k) { return r[L.at(i, j, k)]; },
-        [&](int i, int j, int k, float rv) {
-            const long long c = L.at(i, j, k);
-            r[c] = -md * cell_volume(L, i, j, k) * rv;
-            e[c] = 0.f;
+        L, [&](int i, int j) { return row_base(L, i, j); },
+        [&](const MgRowBase &R, int k) { return r[R.c0 + k]; },
+        [&](const MgRowBase &R, int k, float rv) {
+            r[R.c0 + k] = -md * (R.w01 * L.w[2][k]) * rv;
+            e[R.c0 + k] = 0.f;
         });
 }
 
@@ -308,13 +386,10 @@ k_mg_first(MgLevel L, const float *r, const float *z, float *p, Partials<1> part
     if (st->done) return;
     double acc = 0;
     level_loop<4>(
-        L,
-        [&](int i, int j, int k) {
-            const long long c = L.at(i, j, k);
-            return make_float2(r[c], z[c]);
-        },
-        [&](int i, int j, int k, float2 v) {
-            p[L.at(i, j, k)] = v.y;
+        L, [&](int i, int j) { return L.at(i, j, 0); },
+        [&](long long c0, int k) { return make_float2(r[c0 + k], z[c0 + k]); },
+        [&](long long c0, int k, float2 v) {
+            p[c0 + k] = v.y;
             acc += (double)v.x * (double)v.y;
         });
     double v[1] = {acc};
@@ -330,13 +405,11 @@ __global__ void __launch_bounds__(MG_THREADS)
 k_mg_spmv(MgLevel L, const float *p, float *q, Partials<1> part, KrylovState *st) {
     if (st->done) return;
     double acc = 0;
-    level_loop<2>(
-        L,
-        [&](int i, int j, int k) {
-            return make_float2(mg_apply(L, p, i, j, k), p[L.at(i, j, k)]);
-        },
-        [&](int i, int j, int k, float2 v) {
-            q[L.at(i, j, k)] = v.x;
+    level_loop<4>(
+        L, [&](int i, int j) { return MgRow(L, i, j); },
+        [&](const MgRow &R, int k) { return make_float2(R.apply(L, p, k), p[R.c0 + k]); },
+        [&](const MgRow &R, int k, float2 v) {
+            q[R.c0 + k] = v.x;
             acc += (double)v.y * (double)v.x;
         });
     double v[1] = {acc};
@@ -354,17 +427,17 @@ k_mg_update(MgLevel L, float *e, float *r, const float *p, const float *q, float
     const float a = (float)st->alpha;
     double acc = 0;
     level_loop<4>(
-        L,
-        [&](int i, int j, int k) {
-            const long long c = L.at(i, j, k);
+        L, [&](int i, int j) { return row_base(L, i, j); },
+        [&](const MgRowBase &R, int k) {
+            const long long c = R.c0 + k;
             return make_float4(e[c], p[c], r[c], q[c]);
         },
-        [&](int i, int j, int k, float4 v) {
-            const long long c = L.at(i, j, k);
+        [&](const MgRowBase &R, int k, float4 v) {
+            const long long c = R.c0 + k;
             e[c] = v.x + a * v.y;
             const float rn = v.z - a * v.w;
             r[c] = rn;
-            const double ra = (double)rn / ((double)md * (double)cell_volume(L, i, j, k));
+            const double ra = (double)rn / ((double)md * (double)(R.w01 * L.w[2][k]));
             acc += ra * ra;
         });
     double v[1] = {acc};
@@ -382,12 +455,9 @@ k_mg_rz(MgLevel L, const float *r, const float *z, Partials<1> part, KrylovState
     if (st->done) return;
     double acc = 0;
     level_loop<4>(
-        L,
-        [&](int i, int j, int k) {
-            const long long c = L.at(i, j, k);
-            return make_float2(r[c], z[c]);
-        },
-        [&](int, int, int, float2 v) { acc += (double)v.x * (double)v.y; });
+        L, [&](int i, int j) { return L.at(i, j, 0); },
+        [&](long long c0, int k) { return make_float2(r[c0 + k], z[c0 + k]); },
+        [&](long long, int, float2 v) { acc += (double)v.x * (double)v.y; });
     double v[1] = {acc};
     if (grid_reduce<1>(v, 0u, part) && threadIdx.x == 0) {
         if (!isfinite(v[0])) {
@@ -405,12 +475,9 @@ k_mg_pupdate(MgLevel L, const float *z, float *p, const KrylovState *st) {
     if (st->done) return;
     const float b = (float)st->beta;
     level_loop<4>(
-        L,
-        [&](int i, int j, int k) {
-            const long long c = L.at(i, j, k);
-            return make_float2(z[c], p[c]);
-        },
-        [&](int i, int j, int k, float2 v) { p[L.at(i, j, k)] = v.x + b * v.y; });
+        L, [&](int i, int j) { return L.at(i, j, 0); },
+        [&](long long c0, int k) { return make_float2(z[c0 + k], p[c0 + k]); },
+        [&](long long c0, int k, float2 v) { p[c0 + k] = v.x + b * v.y; });
 }
 
 int blocks_for(long long n, int cap) {
@@ -471,7 +538,7 @@ bool mg_prepare(const MgDev &M) {
 
 void launch_mg_vcycle(const LaunchCtx &L, const MgDev &M, const KrylovState *st) {
     DeviceCycle e{L, M, st};
-    mg_vcycle(e, M.levels, MG_NU);
+    mg_vcycle_nu(e, M.levels, mg_nu);
 }
 
 void launch_mg_begin(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B, double max_diag,

@@ -126,7 +126,7 @@ int mgx_vcycle(void *ctx, const float *f, float *x) {
     if (m->kinv.empty()) return -1;
     m->f[0].assign(f, f + m->L[0].g.total);
     std::fill(m->x[0].begin(), m->x[0].end(), 0.f);
-    mg_vcycle(*m, m->levels, MG_NU);
+    mg_vcycle_nu(*m, m->levels, mg_nu);
     std::copy(m->x[0].begin(), m->x[0].end(), x);
     return 0;
 }
