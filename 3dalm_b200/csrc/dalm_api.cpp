@@ -427,11 +427,21 @@ struct dalm_handle {
             const MgGeometry &G = geo[l];
             MgLevel &v = mgd.L[l];
             v.g = l == 0 ? g : Grid::make(G.n[0] + 2, G.n[1] + 2, G.n[2] + 2, 1);
+            std::vector<float> fcf[3], fw[3];
             for (int a = 0; a < 3; a++) {
                 v.n[a] = G.n[a];
                 v.fac[a] = G.fac[a];
-                v.cf[a] = upload(std::vector<float>(G.cf[a].begin(), G.cf[a].end()));
-                v.w[a] = upload(std::vector<float>(G.w[a].begin(), G.w[a].end()));
+                fcf[a].assign(G.cf[a].begin(), G.cf[a].end());
+                fw[a].assign(G.w[a].begin(), G.w[a].end());
+                v.cf[a] = upload(fcf[a]);
+                v.w[a] = upload(fw[a]);
+            }
+            MgLineTable T;  // the smoother's z-line factors, when the mesh allows
+            if (mg_line_table(v.n, fcf, fw, T)) {
+                v.lcls[0] = upload(T.cls[0]);
+                v.lcls[1] = upload(T.cls[1]);
+                v.lky = T.ky;
+                v.ltab = upload(T.tab);
             }
             if (l > 0) {
                 mgd.x[l] = dalloc<float>((size_t)v.g.total);

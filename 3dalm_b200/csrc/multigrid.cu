@@ -91,6 +91,119 @@ __device__ __forceinline__ MgRowBase row_base(const MgLevel &L, int i, int j) {
     return MgRowBase{L.at(i, j, 0), L.w[0][i] * L.w[1][j]};
 }
 
+// Steps 2 and 3 of the line solve for the lane's rows d[] (right-hand
+// sides in, solution out in x[]): the row coefficients from the column's
+// constants, the lane's Thomas sweeps and the cyclic reduction over lanes.
+template <int R>
+__device__ __forceinline__ void line_solve(float az, float sxy, const float *w2, const float *cf2,
+                                           int nk, int lane, const float (&d)[R], float (&x)[R]) {
+    const unsigned full = 0xffffffffu;
+    float a[R], b[R], c[R];
+#pragma unroll
+    for (int s = 0; s < R; s++) {
+        const int k = R * lane + s;
+        if (k < nk) {
+            const float lo = az * cf2[k], hi = az * cf2[k + 1];
+            a[s] = -lo;
+            b[s] = w2[k] * sxy + lo + hi;
+            c[s] = -hi;
+        } else {
+            a[s] = 0.f;
+            b[s] = 1.f;
+            c[s] = 0.f;
+        }
+    }
+    // 2. rows s < R - 1: x_s = D_s - A_s y_{l-1} - C_s y_l (in e, fa, g)
+    float e[R], fa[R], g[R];
+    float ra = a[R - 1], rb = b[R - 1], rc = c[R - 1], rd = d[R - 1];
+    if (R > 1) {
+#pragma unroll
+        for (int s = 0; s < R - 1; s++) {
+            const float den = s == 0 ? b[0] : b[s] - a[s] * g[s > 0 ? s - 1 : 0];
+            const float q = __fdividef(1.f, den);
+            e[s] = (s == 0 ? d[0] : d[s] - a[s] * e[s > 0 ? s - 1 : 0]) * q;
+            fa[s] = (s == 0 ? a[0] : -a[s] * fa[s > 0 ? s - 1 : 0]) * q;
+            g[s] = c[s] * q;
+        }
+#pragma unroll
+        for (int s = R - 3; s >= 0; s--) {
+            e[s] -= g[s] * e[s + 1];
+            fa[s] -= g[s] * fa[s + 1];
+            g[s] = -g[s] * g[s + 1];
+        }
+        // 3. the last row, with x of the next lane's first row
+        float An = __shfl_down_sync(full, fa[0], 1), Cn = __shfl_down_sync(full, g[0], 1);
+        float Dn = __shfl_down_sync(full, e[0], 1);
+        if (lane == 31) An = Cn = Dn = 0.f;
+        const float al = a[R - 1], cl = c[R - 1];
+        ra = -al * fa[R - 2];
+        rb = b[R - 1] - al * g[R - 2] - cl * An;
+        rc = -cl * Cn;
+        rd = d[R - 1] - al * e[R - 2] - cl * Dn;
+    }
+#pragma unroll
+    for (int delta = 1; delta < 32; delta <<= 1) {
+        float am = __shfl_up_sync(full, ra, delta), bm = __shfl_up_sync(full, rb, delta);
+        float cm = __shfl_up_sync(full, rc, delta), dm = __shfl_up_sync(full, rd, delta);
+        float ap = __shfl_down_sync(full, ra, delta), bp = __shfl_down_sync(full, rb, delta);
+        float cp = __shfl_down_sync(full, rc, delta), dp = __shfl_down_sync(full, rd, delta);
+        if (lane < delta) am = 0.f, bm = 1.f, cm = 0.f, dm = 0.f;  // identity rows
+        if (lane + delta >= 32) ap = 0.f, bp = 1.f, cp = 0.f, dp = 0.f;
+        // approximate quotients (2 ulp): the preconditioner needs no
+        // correctly rounded division
+        const float alpha = -__fdividef(ra, bm), gamma = -__fdividef(rc, bp);
+        rb += alpha * cm + gamma * ap;
+        rd += alpha * dm + gamma * dp;
+        ra = alpha * am;
+        rc = gamma * cp;
+    }
+    const float y = __fdividef(rd, rb);
+    float ym = __shfl_up_sync(full, y, 1);
+    if (lane == 0) ym = 0.f;
+#pragma unroll
+    for (int s = 0; s < R; s++)
+        x[s] = s == R - 1 ? y : e[s < R - 1 ? s : 0] - fa[s < R - 1 ? s : 0] * ym -
+                                    g[s < R - 1 ? s : 0] * y;
+}
+
+// The same with every matrix-only quantity read from the level's factor
+// table (MgLevel::ltab, mglf_* layout; T points at this lane's entry of
+// the column's class): two shuffles and two FMAs per reduction step.
+template <int R>
+__device__ __forceinline__ void line_solve_table(const float *T, int lane, const float (&d)[R],
+                                                 float (&x)[R]) {
+    const unsigned full = 0xffffffffu;
+    float e[R];
+    float rd = d[R - 1];
+    if (R > 1) {
+#pragma unroll
+        for (int s = 0; s < R - 1; s++)
+            e[s] = (s == 0 ? d[0] : d[s] - T[32 * mglf_a(s)] * e[s > 0 ? s - 1 : 0]) *
+                   T[32 * mglf_q(s)];
+#pragma unroll
+        for (int s = R - 3; s >= 0; s--) e[s] -= T[32 * mglf_g(s)] * e[s + 1];
+        float Dn = __shfl_down_sync(full, e[0], 1);
+        if (lane == 31) Dn = 0.f;
+        rd = d[R - 1] - T[32 * mglf_al(R)] * e[R - 2] - T[32 * mglf_cl(R)] * Dn;
+    }
+#pragma unroll
+    for (int t = 0; t < 5; t++) {
+        const int delta = 1 << t;
+        float dm = __shfl_up_sync(full, rd, delta), dp = __shfl_down_sync(full, rd, delta);
+        if (lane < delta) dm = 0.f;
+        if (lane + delta >= 32) dp = 0.f;
+        rd += T[32 * mglf_alpha(R, t)] * dm + T[32 * mglf_gamma(R, t)] * dp;
+    }
+    const float y = rd * T[32 * mglf_invrb(R)];
+    float ym = __shfl_up_sync(full, y, 1);
+    if (lane == 0) ym = 0.f;
+#pragma unroll
+    for (int s = 0; s < R; s++)
+        x[s] = s == R - 1 ? y
+                          : e[s < R - 1 ? s : 0] - T[32 * mglf_xa(s < R - 1 ? s : 0)] * ym -
+                                T[32 * mglf_xc(s < R - 1 ? s : 0)] * y;
+}
+
 // Zebra z-line half-sweep, one warp per column, by the partition method.
 // Lane l owns the R consecutive rows k = R l + s (s < R):
 //  1. the right-hand sides are formed in the coalesced layout k = l + 32 r
@@ -107,7 +220,9 @@ __device__ __forceinline__ MgRowBase row_base(const MgLevel &L, int i, int j) {
 // dominant, which keeps both eliminations stable without pivoting; the result
 // is mg_thomas's up to rounding (this file is compiled with contraction and
 // fast quotients).  Blocks only read columns of the other colour and only
-// write their own.
+// write their own.  FAC: steps 2-3 read the matrix-only quantities from the
+// level's factor table (line_solve_table) instead of forming and
+// eliminating the column's matrix (line_solve).
 //
 // With xc set, the half-sweep also applies the pending prolongation of the
 // coarse correction xc (level C): it reads each interior x or y neighbour
@@ -125,7 +240,7 @@ struct ZlineArgs {
     MgLevel C;
 };
 
-template <int R>
+template <int R, bool FAC>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const KrylovState *st) {
     __shared__ float slab[MG_THREADS / 32][33 * R];
     if (st->done) return;
@@ -133,7 +248,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const Kry
     float *__restrict__ x = A.x;
     const float *__restrict__ f = A.f;
     const float *__restrict__ xc = A.xc;
-    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     float *sl = slab[threadIdx.x >> 5];
     // column n of the colour: i = n / njh, j = 2 (n % njh) + (i + color) % 2
@@ -192,75 +306,23 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const Kry
 #pragma unroll
         for (int r = 0; r < R; r++) sl[lane + 33 * r] = rhs[r];
         __syncwarp();
-        float a[R], b[R], c[R], d[R];
+        float d[R], xs[R];
 #pragma unroll
         for (int s = 0; s < R; s++) {
             const int k = R * lane + s;
             d[s] = sl[k + (k >> 5)];
-            if (k < nk) {
-                const float lo = az * cf2[k], hi = az * cf2[k + 1];
-                a[s] = -lo;
-                b[s] = w2[k] * sxy + lo + hi;
-                c[s] = -hi;
-            } else {
-                a[s] = 0.f;
-                b[s] = 1.f;
-                c[s] = 0.f;
-            }
         }
-        // 2. rows s < R - 1: x_s = D_s - A_s y_{l-1} - C_s y_l (in e, fa, g)
-        float e[R], fa[R], g[R];
-        float ra = a[R - 1], rb = b[R - 1], rc = c[R - 1], rd = d[R - 1];
-        if (R > 1) {
-#pragma unroll
-            for (int s = 0; s < R - 1; s++) {
-                const float den = s == 0 ? b[0] : b[s] - a[s] * g[s > 0 ? s - 1 : 0];
-                const float q = __fdividef(1.f, den);
-                e[s] = (s == 0 ? d[0] : d[s] - a[s] * e[s > 0 ? s - 1 : 0]) * q;
-                fa[s] = (s == 0 ? a[0] : -a[s] * fa[s > 0 ? s - 1 : 0]) * q;
-                g[s] = c[s] * q;
-            }
-#pragma unroll
-            for (int s = R - 3; s >= 0; s--) {
-                e[s] -= g[s] * e[s + 1];
-                fa[s] -= g[s] * fa[s + 1];
-                g[s] = -g[s] * g[s + 1];
-            }
-            // 3. the last row, with x of the next lane's first row
-            float An = __shfl_down_sync(full, fa[0], 1), Cn = __shfl_down_sync(full, g[0], 1);
-            float Dn = __shfl_down_sync(full, e[0], 1);
-            if (lane == 31) An = Cn = Dn = 0.f;
-            const float al = a[R - 1], cl = c[R - 1];
-            ra = -al * fa[R - 2];
-            rb = b[R - 1] - al * g[R - 2] - cl * An;
-            rc = -cl * Cn;
-            rd = d[R - 1] - al * e[R - 2] - cl * Dn;
-        }
-#pragma unroll
-        for (int delta = 1; delta < 32; delta <<= 1) {
-            float am = __shfl_up_sync(full, ra, delta), bm = __shfl_up_sync(full, rb, delta);
-            float cm = __shfl_up_sync(full, rc, delta), dm = __shfl_up_sync(full, rd, delta);
-            float ap = __shfl_down_sync(full, ra, delta), bp = __shfl_down_sync(full, rb, delta);
-            float cp = __shfl_down_sync(full, rc, delta), dp = __shfl_down_sync(full, rd, delta);
-            if (lane < delta) am = 0.f, bm = 1.f, cm = 0.f, dm = 0.f;  // identity rows
-            if (lane + delta >= 32) ap = 0.f, bp = 1.f, cp = 0.f, dp = 0.f;
-            // approximate quotients (2 ulp): the preconditioner needs no
-            // correctly rounded division
-            const float alpha = -__fdividef(ra, bm), gamma = -__fdividef(rc, bp);
-            rb += alpha * cm + gamma * ap;
-            rd += alpha * dm + gamma * dp;
-            ra = alpha * am;
-            rc = gamma * cp;
-        }
-        const float y = __fdividef(rd, rb);
-        float ym = __shfl_up_sync(full, y, 1);
-        if (lane == 0) ym = 0.f;
-        // 4. expand and store through the slab
+        if (FAC)
+            line_solve_table<R>(L.ltab + (size_t)(L.lcls[0][i] * L.lky + L.lcls[1][j]) *
+                                             mglf_count(R) * 32 + lane,
+                                lane, d, xs);
+        else
+            line_solve<R>(az, sxy, w2, cf2, nk, lane, d, xs);
+        // 4. store through the slab
 #pragma unroll
         for (int s = 0; s < R; s++) {
             const int k = R * lane + s;
-            sl[k + (k >> 5)] = s == R - 1 ? y : e[s < R - 1 ? s : 0] - fa[s < R - 1 ? s : 0] * ym -
-                                                    g[s < R - 1 ? s : 0] * y;
+            sl[k + (k >> 5)] = xs[s];
         }
         __syncwarp();
 #pragma unroll
@@ -276,7 +338,10 @@ constexpr int ZL_MAX_R = 8;
 
 template <int R>
 void zline_launch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st, int blocks) {
-    k_mg_smooth<R><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+    if (a.L.ltab)
+        k_mg_smooth<R, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+    else
+        k_mg_smooth<R, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
 }
 
 void zline_dispatch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st) {

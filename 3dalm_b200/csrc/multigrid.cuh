@@ -50,11 +50,40 @@ struct MgLevel {
     int fac[3];          // children per coarse cell along each axis (1 or 2); finest: 1
     const float *cf[3];  // face conductances, [n + 1]
     const float *w[3];   // cell widths, [n]
+    // z-line factor table (or null): the line matrix of column (i, j) depends
+    // on (i, j) only through (w0[i], cf0[i + 1], cf0[i]) and (w1[j], cf1[j + 1],
+    // cf1[j]); lcls[0][i] and lcls[1][j] number those triples, and column
+    // (i, j) uses class lcls[0][i] * lky + lcls[1][j] of ltab (layout: mglf_*)
+    const int *lcls[2] = {nullptr, nullptr};
+    int lky = 0;
+    const float *ltab = nullptr;
     DALM_HD long long at(int i, int j, int k) const {
         return g.at(i + g.gc, j + g.gc, k + g.gc);
     }
     DALM_HD long long cells() const { return (long long)n[0] * n[1] * n[2]; }
 };
+
+// Field layout of the z-line factor table, per class [field][lane] (32
+// lanes): the partition-method line solve of k_mg_smooth with every
+// quantity that depends only on the line matrix precomputed, for R rows
+// per lane (rows R l + s):
+//   Q(s), A(s)   forward sweep  e_s = (d_s - A(s) e_{s-1}) Q(s)   (s < R-1)
+//   G(s)         back sweep     e_s -= G(s) e_{s+1}
+//   XA(s), XC(s) expansion      x_s = e_s - XA(s) y_{l-1} - XC(s) y_l
+//   AL, CL       the last row's couplings (R > 1)
+//   ALPHA(t), GAMMA(t)  cyclic-reduction step t (stride 2^t) multipliers
+//   INVRB        1 / the reduced diagonal after the reduction
+DALM_HD constexpr int mglf_q(int s) { return 5 * s; }
+DALM_HD constexpr int mglf_a(int s) { return 5 * s + 1; }
+DALM_HD constexpr int mglf_g(int s) { return 5 * s + 2; }
+DALM_HD constexpr int mglf_xa(int s) { return 5 * s + 3; }
+DALM_HD constexpr int mglf_xc(int s) { return 5 * s + 4; }
+DALM_HD constexpr int mglf_al(int R) { return 5 * (R - 1); }
+DALM_HD constexpr int mglf_cl(int R) { return 5 * (R - 1) + 1; }
+DALM_HD constexpr int mglf_alpha(int R, int t) { return 5 * (R - 1) + (R > 1 ? 2 : 0) + 2 * t; }
+DALM_HD constexpr int mglf_gamma(int R, int t) { return mglf_alpha(R, t) + 1; }
+DALM_HD constexpr int mglf_invrb(int R) { return mglf_alpha(R, 5); }
+DALM_HD constexpr int mglf_count(int R) { return mglf_invrb(R) + 1; }
 
 // Sum over the faces of cell (i,j,k) of area * conductance * x_neighbour
 // (x = 0 beyond the boundary, where the guide cells hold zeros), and the

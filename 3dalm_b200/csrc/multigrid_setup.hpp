@@ -3,9 +3,12 @@
 // inverse of the coarsest operator.  FP64 here; the device stores FP32.
 #pragma once
 
+#include <array>
 #include <cmath>
 #include <stdexcept>
 #include <vector>
+
+#include "multigrid.cuh"
 
 namespace dalm {
 
@@ -126,6 +129,135 @@ inline std::vector<double> mg_spd_inverse(std::vector<double> A, long long N) {
         }
     }
     return X;
+}
+
+// Z-line factor table of a level (MgLevel::ltab): the classes of columns
+// with equal line matrices and, per class, the matrix-only quantities of the
+// partition-method solve (mglf_* layout), computed in FP64 from the FP32
+// level arrays the device holds and the same formulas as k_mg_smooth's
+// generic path.  False (no table) when the columns are longer than 256
+// cells or there are more than MG_MAX_LINE_CLASSES classes (a mesh that is
+// not uniform in x or y); the smoother then forms and eliminates each
+// column's matrix itself.
+constexpr int MG_MAX_LINE_CLASSES = 64;
+
+struct MgLineTable {
+    std::vector<int> cls[2];
+    int ky = 0, nclass = 0, nf = 0;
+    std::vector<float> tab;
+};
+
+inline bool mg_line_table(const int (&n)[3], const std::vector<float> (&cf)[3],
+                          const std::vector<float> (&w)[3], MgLineTable &T) {
+    const int nk = n[2], R = (nk + 31) / 32;
+    if (R < 1 || R > 8) return false;
+    std::vector<std::array<float, 3>> keys[2];
+    for (int a = 0; a < 2; a++) {
+        T.cls[a].assign(n[a], 0);
+        for (int q = 0; q < n[a]; q++) {
+            const std::array<float, 3> key = {w[a][q], cf[a][q + 1], cf[a][q]};
+            size_t c = 0;
+            while (c < keys[a].size() && keys[a][c] != key) c++;
+            if (c == keys[a].size()) {
+                if ((int)keys[a].size() >= MG_MAX_LINE_CLASSES) return false;
+                keys[a].push_back(key);
+            }
+            T.cls[a][q] = (int)c;
+        }
+    }
+    T.ky = (int)keys[1].size();
+    T.nclass = (int)keys[0].size() * T.ky;
+    if (T.nclass > MG_MAX_LINE_CLASSES) return false;
+    T.nf = mglf_count(R);
+    T.tab.assign((size_t)T.nclass * T.nf * 32, 0.f);
+    const int N = 32 * R;
+    std::vector<double> A(N), B(N), C(N), q(N), fa(N), g(N), xa(N), xc(N);
+    double ra[32], rb[32], rc[32];
+    for (int cx = 0; cx < (int)keys[0].size(); cx++)
+        for (int cy = 0; cy < T.ky; cy++) {
+            float *tab = T.tab.data() + (size_t)(cx * T.ky + cy) * T.nf * 32;
+            auto put = [&](int field, int lane, double v) { tab[field * 32 + lane] = (float)v; };
+            const double wi = keys[0][cx][0], xe = keys[0][cx][1], xw = keys[0][cx][2];
+            const double wj = keys[1][cy][0], yn = keys[1][cy][1], ys = keys[1][cy][2];
+            const double az = wi * wj, sxy = wj * (xe + xw) + wi * (yn + ys);
+            for (int k = 0; k < N; k++) {
+                if (k < nk) {
+                    const double lo = az * cf[2][k], hi = az * cf[2][k + 1];
+                    A[k] = -lo;
+                    B[k] = w[2][k] * sxy + lo + hi;
+                    C[k] = -hi;
+                } else {
+                    A[k] = 0;
+                    B[k] = 1;
+                    C[k] = 0;
+                }
+            }
+            // each lane's first R - 1 rows: forward, then back sweep
+            for (int l = 0; l < 32; l++) {
+                const int k0 = R * l;
+                for (int s = 0; s + 1 < R; s++) {
+                    const int k = k0 + s;
+                    const double den = s == 0 ? B[k] : B[k] - A[k] * g[k - 1];
+                    q[k] = 1.0 / den;
+                    fa[k] = (s == 0 ? A[k] : -A[k] * fa[k - 1]) * q[k];
+                    g[k] = C[k] * q[k];
+                    put(mglf_q(s), l, q[k]);
+                    put(mglf_a(s), l, A[k]);
+                    put(mglf_g(s), l, g[k]);
+                }
+                for (int s = R - 2; s >= 0; s--) {
+                    const int k = k0 + s;
+                    if (s == R - 2) {
+                        xa[k] = fa[k];
+                        xc[k] = g[k];
+                    } else {
+                        xa[k] = fa[k] - g[k] * xa[k + 1];
+                        xc[k] = -g[k] * xc[k + 1];
+                    }
+                    put(mglf_xa(s), l, xa[k]);
+                    put(mglf_xc(s), l, xc[k]);
+                }
+            }
+            // the lanes' last rows, in the segment ends y_l alone
+            for (int l = 0; l < 32; l++) {
+                const int kl = R * l + R - 1;
+                if (R == 1) {
+                    ra[l] = A[kl];
+                    rb[l] = B[kl];
+                    rc[l] = C[kl];
+                    continue;
+                }
+                const double An = l < 31 ? xa[R * (l + 1)] : 0.0, Cn = l < 31 ? xc[R * (l + 1)] : 0.0;
+                ra[l] = -A[kl] * xa[kl - 1];
+                rb[l] = B[kl] - A[kl] * xc[kl - 1] - C[kl] * An;
+                rc[l] = -C[kl] * Cn;
+                put(mglf_al(R), l, A[kl]);
+                put(mglf_cl(R), l, C[kl]);
+            }
+            // parallel cyclic reduction over the lanes (identity rows outside)
+            for (int t = 0; t < 5; t++) {
+                const int d = 1 << t;
+                double na[32], nb[32], nc[32];
+                for (int l = 0; l < 32; l++) {
+                    const bool m = l >= d, p = l + d < 32;
+                    const double am = m ? ra[l - d] : 0, bm = m ? rb[l - d] : 1, cm = m ? rc[l - d] : 0;
+                    const double ap = p ? ra[l + d] : 0, bp = p ? rb[l + d] : 1, cp = p ? rc[l + d] : 0;
+                    const double alpha = -ra[l] / bm, gamma = -rc[l] / bp;
+                    put(mglf_alpha(R, t), l, alpha);
+                    put(mglf_gamma(R, t), l, gamma);
+                    nb[l] = rb[l] + alpha * cm + gamma * ap;
+                    na[l] = alpha * am;
+                    nc[l] = gamma * cp;
+                }
+                for (int l = 0; l < 32; l++) {
+                    ra[l] = na[l];
+                    rb[l] = nb[l];
+                    rc[l] = nc[l];
+                }
+            }
+            for (int l = 0; l < 32; l++) put(mglf_invrb(R), l, 1.0 / rb[l]);
+        }
+    return true;
 }
 
 }  // namespace dalm

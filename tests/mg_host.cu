@@ -6,6 +6,7 @@
 // functions (multigrid.cuh) in plain loops, so the CPU test suite can check
 // the operator against the oracle's matrix and the V-cycle's symmetry and
 // convergence.  Level 0 uses the solver's padded layout (2 guide cells).
+#include <algorithm>
 #include <vector>
 
 #include "../3dalm_b200/csrc/multigrid.cuh"
@@ -129,6 +130,34 @@ int mgx_vcycle(void *ctx, const float *f, float *x) {
     mg_vcycle_nu(*m, m->levels, mg_nu);
     std::copy(m->x[0].begin(), m->x[0].end(), x);
     return 0;
+}
+
+// The level's FP32 arrays as the device holds them (cf: n + 1, w: n).
+void mgx_level_arrays(void *ctx, int l, int a, float *cf, float *w) {
+    HostMg *m = (HostMg *)ctx;
+    std::copy(m->cf[a][l].begin(), m->cf[a][l].end(), cf);
+    std::copy(m->w[a][l].begin(), m->w[a][l].end(), w);
+}
+
+// The smoother's z-line factor table of level l (mg_line_table): info gets
+// {built, ky, nclass, nf}; with non-null outputs also the classes and table.
+void mgx_line_table(void *ctx, int l, int *info, int *cls_x, int *cls_y, float *tab) {
+    HostMg *m = (HostMg *)ctx;
+    std::vector<float> cf[3], w[3];
+    for (int a = 0; a < 3; a++) {
+        cf[a] = m->cf[a][l];
+        w[a] = m->w[a][l];
+    }
+    MgLineTable T;
+    const bool ok = mg_line_table(m->L[l].n, cf, w, T);
+    info[0] = ok ? 1 : 0;
+    info[1] = T.ky;
+    info[2] = T.nclass;
+    info[3] = T.nf;
+    if (!ok) return;
+    if (cls_x) std::copy(T.cls[0].begin(), T.cls[0].end(), cls_x);
+    if (cls_y) std::copy(T.cls[1].begin(), T.cls[1].end(), cls_y);
+    if (tab) std::copy(T.tab.begin(), T.tab.end(), tab);
 }
 
 }  // extern "C"

@@ -42,6 +42,9 @@ def harness():
     lib.mgx_total.argtypes = [C.c_void_p]
     lib.mgx_apply.argtypes = [C.c_void_p, PF, PF]
     lib.mgx_vcycle.argtypes = [C.c_void_p, PF, PF]
+    PI = C.POINTER(C.c_int)
+    lib.mgx_level_arrays.argtypes = [C.c_void_p, C.c_int, C.c_int, PF, PF]
+    lib.mgx_line_table.argtypes = [C.c_void_p, C.c_int, PI, PI, PI, PF]
     return lib
 
 
@@ -88,6 +91,31 @@ class HostMg:
         x = np.zeros_like(f)
         assert self.lib.mgx_vcycle(self.h, f.ctypes.data_as(PF), x.ctypes.data_as(PF)) == 0
         return self.unpad(x)
+
+    def level_arrays(self, l):
+        """(cf, w) per axis of level l, FP32 as the device holds them"""
+        out = []
+        for a in range(3):
+            n = self.levels[l][a]
+            cf, w = np.zeros(n + 1, np.float32), np.zeros(n, np.float32)
+            self.lib.mgx_level_arrays(self.h, l, a, cf.ctypes.data_as(PF), w.ctypes.data_as(PF))
+            out.append((cf.astype(np.float64), w.astype(np.float64)))
+        return out
+
+    def line_table(self, l):
+        """the smoother's z-line factor table of level l, or None"""
+        info = np.zeros(4, np.int32)
+        PI = C.POINTER(C.c_int)
+        self.lib.mgx_line_table(self.h, l, info.ctypes.data_as(PI), None, None, None)
+        if not info[0]:
+            return None
+        n = self.levels[l]
+        cx, cy = np.zeros(n[0], np.int32), np.zeros(n[1], np.int32)
+        tab = np.zeros(info[2] * info[3] * 32, np.float32)
+        self.lib.mgx_line_table(self.h, l, info.ctypes.data_as(PI), cx.ctypes.data_as(PI),
+                                cy.ctypes.data_as(PI), tab.ctypes.data_as(PF))
+        return {"ky": int(info[1]), "nclass": int(info[2]), "nf": int(info[3]), "cls_x": cx,
+                "cls_y": cy, "tab": tab.reshape(info[2], info[3], 32).astype(np.float64)}
 
     def close(self):
         self.lib.mgx_destroy(self.h)
@@ -176,5 +204,97 @@ def test_preconditioned_cg_converges_in_few_iterations(n):
             _, it_plain = pcg(mg.apply, lambda r: r, f, 1e-5, 5000)
             print("unpreconditioned CG:", it_plain)
             assert it_plain > 5 * it
+    finally:
+        mg.close()
+
+
+# field layout of the factor table (multigrid.cuh, mglf_*)
+def _f_q(s): return 5 * s
+def _f_a(s): return 5 * s + 1
+def _f_g(s): return 5 * s + 2
+def _f_xa(s): return 5 * s + 3
+def _f_xc(s): return 5 * s + 4
+def _f_al(R): return 5 * (R - 1)
+def _f_cl(R): return 5 * (R - 1) + 1
+def _f_alpha(R, t): return 5 * (R - 1) + (2 if R > 1 else 0) + 2 * t
+def _f_gamma(R, t): return _f_alpha(R, t) + 1
+def _f_invrb(R): return _f_alpha(R, 5)
+
+
+def line_solve_table(T, R, d):
+    """k_mg_smooth's table path (line_solve_table) lane by lane: T[field][lane],
+    d[lane, s] the right-hand sides of rows R lane + s"""
+    lanes = np.arange(32)
+    e = np.zeros((32, R))
+    if R > 1:
+        for s in range(R - 1):
+            e[:, s] = (d[:, 0] if s == 0 else d[:, s] - T[_f_a(s)] * e[:, s - 1]) * T[_f_q(s)]
+        for s in range(R - 3, -1, -1):
+            e[:, s] -= T[_f_g(s)] * e[:, s + 1]
+        dn = np.roll(e[:, 0], -1)
+        dn[31] = 0
+        rd = d[:, R - 1] - T[_f_al(R)] * e[:, R - 2] - T[_f_cl(R)] * dn
+    else:
+        rd = d[:, 0].copy()
+    for t in range(5):
+        dl = 1 << t
+        dm, dp = np.roll(rd, dl), np.roll(rd, -dl)
+        dm[lanes < dl] = 0
+        dp[lanes + dl >= 32] = 0
+        rd = rd + T[_f_alpha(R, t)] * dm + T[_f_gamma(R, t)] * dp
+    y = rd * T[_f_invrb(R)]
+    ym = np.roll(y, 1)
+    ym[0] = 0
+    x = np.zeros((32, R))
+    x[:, R - 1] = y
+    for s in range(R - 1):
+        x[:, s] = e[:, s] - T[_f_xa(s)] * ym - T[_f_xc(s)] * y
+    return x
+
+
+@pytest.mark.parametrize("n", [(40, 20, 20), (48, 20, 72), (64, 32, 128), (16, 8, 200)])
+def test_line_factor_table_solves_every_column(n):
+    """On every level, the smoother's factored z-line solve (the table from
+    the product's set-up, applied as the kernel's table path does) matches a
+    dense solve of each column's line matrix, for columns of every class."""
+    cg = casegen()
+    mesh = cg.make_mesh(*n)
+    mg = HostMg(mesh.x, mesh.y, mesh.z, mesh.gc)
+    rng = np.random.default_rng(3)
+    try:
+        for l, (n0, n1, nk) in enumerate(mg.levels):
+            tb = mg.line_table(l)
+            assert tb is not None, "uniform x and y spacing: few classes"
+            assert tb["nclass"] <= 16, tb["nclass"]
+            R = (nk + 31) // 32
+            (cf0, w0), (cf1, w1), (cf2, w2) = mg.level_arrays(l)
+            for i in sorted({0, n0 - 1, n0 // 2}):
+                for j in sorted({0, n1 - 1, n1 // 2}):
+                    az = w0[i] * w1[j]
+                    sxy = w1[j] * (cf0[i + 1] + cf0[i]) + w0[i] * (cf1[j + 1] + cf1[j])
+                    lo, hi = az * cf2[:nk], az * cf2[1:nk + 1]
+                    M = np.diag(w2 * sxy + lo + hi) - np.diag(lo[1:], -1) - np.diag(hi[:-1], 1)
+                    rhs = rng.standard_normal(nk)
+                    ref = np.linalg.solve(M, rhs)
+                    d = np.zeros(32 * R)
+                    d[:nk] = rhs
+                    T = tb["tab"][tb["cls_x"][i] * tb["ky"] + tb["cls_y"][j]]
+                    got = line_solve_table(T, R, d.reshape(32, R)).reshape(-1)[:nk]
+                    err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
+                    assert err < 2e-5, (l, i, j, err)
+    finally:
+        mg.close()
+
+
+def test_line_factor_table_falls_back_on_irregular_meshes():
+    """x spacing with more distinct cells than the table takes: no table,
+    the smoother forms each column's matrix itself."""
+    cg = casegen()
+    mesh = cg.make_mesh(160, 8, 16)
+    x = mesh.x.copy()
+    x[2:-2] += 0.01 * np.sin(np.arange(len(x) - 4) ** 1.5)  # every x cell different
+    mg = HostMg(x, mesh.y, mesh.z, mesh.gc)
+    try:
+        assert mg.line_table(0) is None
     finally:
         mg.close()
