@@ -436,8 +436,11 @@ struct dalm_handle {
                 v.cf[a] = upload(fcf[a]);
                 v.w[a] = upload(fw[a]);
             }
-            MgLineTable T;  // the smoother's z-line factors, when the mesh allows
-            if (mg_line_table(v.n, fcf, fw, T)) {
+            // the smoother's z-line factors on the two finest levels, when the
+            // mesh allows (on the coarser, latency-bound levels the table's
+            // loads cost more than the elimination they save: measured on C4)
+            MgLineTable T;
+            if (l < 2 && mg_line_table(v.n, fcf, fw, T)) {
                 v.lcls[0] = upload(T.cls[0]);
                 v.lcls[1] = upload(T.cls[1]);
                 v.lky = T.ky;
