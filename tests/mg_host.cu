@@ -59,6 +59,58 @@ struct HostMg {
     }
 };
 
+// The V-cycle as the CUDA executor (DeviceCycle in multigrid.cu) runs it:
+// the restriction leaves out the children of the colour smoothed last, and
+// each prolongation is not applied as a pass but by the next half-sweep,
+// which reads its interior x/y neighbours as x + the parent's correction.
+struct HostMgFolded {
+    HostMg &m;
+    int last_color[MG_MAX_LEVELS] = {};
+    bool pending[MG_MAX_LEVELS] = {};
+    void smooth(int l, int color, bool zero) {
+        const MgLevel &v = m.L[l];
+        std::vector<float> &x = m.x[l];
+        const long long half = (long long)v.n[0] * ((v.n[1] + 1) / 2);
+        for (long long n = 0; n < half; n++) {
+            int i, j;
+            if (!mg_color_column(v, n, color, i, j)) continue;
+            const long long c0 = v.at(i, j, 0);
+            for (int k = 0; k < v.n[2]; k++) {
+                const long long c = c0 + k;
+                float r = m.f[l][c];
+                if (!zero) {
+                    auto nb = [&](int ii, int jj, long long q) {
+                        float val = x[q];
+                        if (pending[l] && ii >= 0 && ii < v.n[0] && jj >= 0 && jj < v.n[1]) {
+                            const MgLevel &C = m.L[l + 1];
+                            val += m.x[l + 1][C.at(ii / C.fac[0], jj / C.fac[1], k / C.fac[2])];
+                        }
+                        return val;
+                    };
+                    const float wi = v.w[0][i], wj = v.w[1][j];
+                    const float ax = wj * v.w[2][k], ay = wi * v.w[2][k];
+                    r += ax * (v.cf[0][i + 1] * nb(i + 1, j, c + v.g.sx) + v.cf[0][i] * nb(i - 1, j, c - v.g.sx)) +
+                         ay * (v.cf[1][j + 1] * nb(i, j + 1, c + v.g.sy) + v.cf[1][j] * nb(i, j - 1, c - v.g.sy));
+                }
+                x[c] = r;
+            }
+            mg_thomas(v, i, j, x.data() + c0, m.cp[l].data() + c0, 1);
+        }
+        pending[l] = false;
+        last_color[l] = color;
+    }
+    void restrict(int l) {
+        const MgLevel &c = m.L[l + 1];
+        for (int I = 0; I < c.n[0]; I++)
+            for (int J = 0; J < c.n[1]; J++)
+                for (int K = 0; K < c.n[2]; K++)
+                    m.f[l + 1][c.at(I, J, K)] = mg_restrict_sum(m.L[l], c, m.x[l].data(), m.f[l].data(),
+                                                                I, J, K, last_color[l]);
+    }
+    void coarse() { m.coarse(); }
+    void prolong(int l) { pending[l] = true; }
+};
+
 }  // namespace
 
 extern "C" {
@@ -158,6 +210,18 @@ void mgx_line_table(void *ctx, int l, int *info, int *cls_x, int *cls_y, float *
     if (cls_x) std::copy(T.cls[0].begin(), T.cls[0].end(), cls_x);
     if (cls_y) std::copy(T.cls[1].begin(), T.cls[1].end(), cls_y);
     if (tab) std::copy(T.tab.begin(), T.tab.end(), tab);
+}
+
+// x = the V-cycle as the CUDA executor folds it (HostMgFolded)
+int mgx_vcycle_folded(void *ctx, const float *f, float *x) {
+    HostMg *m = (HostMg *)ctx;
+    if (m->kinv.empty()) return -1;
+    m->f[0].assign(f, f + m->L[0].g.total);
+    std::fill(m->x[0].begin(), m->x[0].end(), 0.f);
+    HostMgFolded e{*m};
+    mg_vcycle_nu(e, m->levels, mg_nu);
+    std::copy(m->x[0].begin(), m->x[0].end(), x);
+    return 0;
 }
 
 }  // extern "C"

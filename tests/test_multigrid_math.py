@@ -43,6 +43,7 @@ def harness():
     lib.mgx_apply.argtypes = [C.c_void_p, PF, PF]
     lib.mgx_vcycle.argtypes = [C.c_void_p, PF, PF]
     PI = C.POINTER(C.c_int)
+    lib.mgx_vcycle_folded.argtypes = [C.c_void_p, PF, PF]
     lib.mgx_level_arrays.argtypes = [C.c_void_p, C.c_int, C.c_int, PF, PF]
     lib.mgx_line_table.argtypes = [C.c_void_p, C.c_int, PI, PI, PI, PF]
     return lib
@@ -90,6 +91,12 @@ class HostMg:
         f = self.pad(v)
         x = np.zeros_like(f)
         assert self.lib.mgx_vcycle(self.h, f.ctypes.data_as(PF), x.ctypes.data_as(PF)) == 0
+        return self.unpad(x)
+
+    def vcycle_folded(self, v):
+        f = self.pad(v)
+        x = np.zeros_like(f)
+        assert self.lib.mgx_vcycle_folded(self.h, f.ctypes.data_as(PF), x.ctypes.data_as(PF)) == 0
         return self.unpad(x)
 
     def level_arrays(self, l):
@@ -296,5 +303,34 @@ def test_line_factor_table_falls_back_on_irregular_meshes():
     mg = HostMg(x, mesh.y, mesh.z, mesh.gc)
     try:
         assert mg.line_table(0) is None
+    finally:
+        mg.close()
+
+
+@pytest.mark.parametrize("n", [(40, 20, 20), (48, 20, 72), (64, 32, 16)])
+def test_folded_vcycle_equals_the_plain_one(n):
+    """The CUDA executor's two shortcuts keep the V-cycle's operator: the
+    restriction without the children of the colour smoothed last (their
+    lines were just solved exactly, so their residual is zero) and the
+    prolongation applied by the next half-sweep's neighbour reads (the two
+    half-sweeps after it overwrite both colours) give the plain V-cycle's
+    result up to FP32 rounding (the dropped residuals are rounding-level, and
+    a V-cycle over z-merged levels amplifies rounding to ~1e-5), and a
+    symmetric positive operator as conjugate gradients need."""
+    cg = casegen()
+    mesh = cg.make_mesh(*n)
+    mg = HostMg(mesh.x, mesh.y, mesh.z, mesh.gc)
+    try:
+        rng = np.random.default_rng(4)
+        for _ in range(2):
+            f = rng.standard_normal(mg.n)
+            a, b = mg.vcycle(f), mg.vcycle_folded(f)
+            err = np.linalg.norm(a - b) / np.linalg.norm(a)
+            print(n, "levels", mg.levels, "folded vs plain V-cycle:", err)
+            assert err < 1e-4
+        u, v = rng.standard_normal(mg.n), rng.standard_normal(mg.n)
+        Mu, Mv = mg.vcycle_folded(u), mg.vcycle_folded(v)
+        assert abs(np.sum(u * Mv) - np.sum(Mu * v)) <= 1e-4 * np.sqrt(np.sum(u * Mu) * np.sum(v * Mv))
+        assert np.sum(u * Mu) > 0 and np.sum(v * Mv) > 0
     finally:
         mg.close()
