@@ -5,6 +5,7 @@
 // of iterations can be enqueued (and replayed as CUDA graphs) ahead of the
 // host's convergence check.
 #include <cfloat>
+#include <cstdint>
 
 #include "multigrid.cuh"
 #include "poisson.cuh"
@@ -204,6 +205,39 @@ __device__ __forceinline__ void line_solve_table(const float *T, int lane, const
                                 T[32 * mglf_xc(s < R - 1 ? s : 0)] * y;
 }
 
+// R consecutive floats at p (VEC path: p is 4R-byte aligned)
+template <int R>
+__device__ __forceinline__ void load_seg(const float *p, float (&v)[R]) {
+    if constexpr (R == 8) {
+        const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    } else if constexpr (R == 4) {
+        const float4 a = *reinterpret_cast<const float4 *>(p);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+    } else if constexpr (R == 2) {
+        const float2 a = *reinterpret_cast<const float2 *>(p);
+        v[0] = a.x, v[1] = a.y;
+    } else {
+#pragma unroll
+        for (int s = 0; s < R; s++) v[s] = p[s];
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void store_seg(float *p, const float (&v)[R]) {
+    if constexpr (R == 8) {
+        reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4 *>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+    } else if constexpr (R == 4) {
+        *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (R == 2) {
+        *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+    } else {
+#pragma unroll
+        for (int s = 0; s < R; s++) p[s] = v[s];
+    }
+}
+
 // Zebra z-line half-sweep, one warp per column, by the partition method.
 // Lane l owns the R consecutive rows k = R l + s (s < R):
 //  1. the right-hand sides are formed in the coalesced layout k = l + 32 r
@@ -222,7 +256,10 @@ __device__ __forceinline__ void line_solve_table(const float *T, int lane, const
 // fast quotients).  Blocks only read columns of the other colour and only
 // write their own.  FAC: steps 2-3 read the matrix-only quantities from the
 // level's factor table (line_solve_table) instead of forming and
-// eliminating the column's matrix (line_solve).
+// eliminating the column's matrix (line_solve).  VEC (columns of exactly
+// 32 R cells, R = 1, 2, 4, 8, on rows whose k = 0 is 32-byte aligned, which
+// Grid's layout gives every interior row): each lane loads and stores its
+// own R rows with vector accesses, and no slab is needed.
 //
 // With xc set, the half-sweep also applies the pending prolongation of the
 // coarse correction xc (level C): it reads each interior x or y neighbour
@@ -240,7 +277,7 @@ struct ZlineArgs {
     MgLevel C;
 };
 
-template <int R, bool FAC>
+template <int R, bool FAC, bool VEC>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const KrylovState *st) {
     __shared__ float slab[MG_THREADS / 32][33 * R];
     if (st->done) return;
@@ -281,36 +318,65 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const Kry
         // the column and its x and y neighbours, from k = 0
         const float *fr = f + c0, *xre = x + c0 + L.g.sx, *xrw = x + c0 - L.g.sx,
                     *xrn = x + c0 + L.g.sy, *xrs = x + c0 - L.g.sy;
-        // all of the column's loads first, then the slab
-        float rhs[R];
+        float d[R], xs[R];
+        if (VEC) {
+            // this lane's rows k = R lane + s, with vector loads
+            const int k0 = R * lane;
+            float vf[R], vw2[R], ve[R], vw[R], vn[R], vs[R];
+            load_seg<R>(fr + k0, vf);
+            if (!zero) {
+                load_seg<R>(w2 + k0, vw2);
+                load_seg<R>(xre + k0, ve);
+                load_seg<R>(xrw + k0, vw);
+                load_seg<R>(xrn + k0, vn);
+                load_seg<R>(xrs + k0, vs);
+                if (xc) {
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int k = lane + 32 * r;
-            rhs[r] = 0.f;
-            if (k < nk) {
-                rhs[r] = fr[k];
-                if (!zero) {
-                    float ve = xre[k], vw = xrw[k], vn = xrn[k], vs = xrs[k];
-                    if (xc) {
-                        const int K = k >> kshift;
-                        if (pe >= 0) ve += xc[pe + K];
-                        if (pw >= 0) vw += xc[pw + K];
-                        if (pn >= 0) vn += xc[pn + K];
-                        if (ps >= 0) vs += xc[ps + K];
+                    for (int q = 0; q < R; q++) {
+                        const int K = (k0 + q) >> kshift;
+                        if (pe >= 0) ve[q] += xc[pe + K];
+                        if (pw >= 0) vw[q] += xc[pw + K];
+                        if (pn >= 0) vn[q] += xc[pn + K];
+                        if (ps >= 0) vs[q] += xc[ps + K];
                     }
-                    rhs[r] += w2[k] * (wj * (xe * ve + xw * vw) + wi * (yn * vn + ys * vs));
                 }
             }
-        }
-        __syncwarp();  // the previous column's reads of the slab are done
 #pragma unroll
-        for (int r = 0; r < R; r++) sl[lane + 33 * r] = rhs[r];
-        __syncwarp();
-        float d[R], xs[R];
+            for (int q = 0; q < R; q++)
+                d[q] = zero ? vf[q]
+                            : vf[q] + vw2[q] * (wj * (xe * ve[q] + xw * vw[q]) +
+                                                wi * (yn * vn[q] + ys * vs[q]));
+        } else {
+            // all of the column's loads first, then the slab
+            float rhs[R];
 #pragma unroll
-        for (int s = 0; s < R; s++) {
-            const int k = R * lane + s;
-            d[s] = sl[k + (k >> 5)];
+            for (int r = 0; r < R; r++) {
+                const int k = lane + 32 * r;
+                rhs[r] = 0.f;
+                if (k < nk) {
+                    rhs[r] = fr[k];
+                    if (!zero) {
+                        float ve = xre[k], vw = xrw[k], vn = xrn[k], vs = xrs[k];
+                        if (xc) {
+                            const int K = k >> kshift;
+                            if (pe >= 0) ve += xc[pe + K];
+                            if (pw >= 0) vw += xc[pw + K];
+                            if (pn >= 0) vn += xc[pn + K];
+                            if (ps >= 0) vs += xc[ps + K];
+                        }
+                        rhs[r] += w2[k] * (wj * (xe * ve + xw * vw) + wi * (yn * vn + ys * vs));
+                    }
+                }
+            }
+            __syncwarp();  // the previous column's reads of the slab are done
+#pragma unroll
+            for (int r = 0; r < R; r++) sl[lane + 33 * r] = rhs[r];
+            __syncwarp();
+#pragma unroll
+            for (int s = 0; s < R; s++) {
+                const int k = R * lane + s;
+                d[s] = sl[k + (k >> 5)];
+            }
         }
         if (FAC)
             line_solve_table<R>(L.ltab + (size_t)(L.lcls[0][i] * L.lky + L.lcls[1][j]) *
@@ -318,17 +384,21 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const Kry
                                 lane, d, xs);
         else
             line_solve<R>(az, sxy, w2, cf2, nk, lane, d, xs);
-        // 4. store through the slab
+        // 4. store (through the slab into the coalesced layout unless VEC)
+        if (VEC) {
+            store_seg<R>(x + c0 + R * lane, xs);
+        } else {
 #pragma unroll
-        for (int s = 0; s < R; s++) {
-            const int k = R * lane + s;
-            sl[k + (k >> 5)] = xs[s];
-        }
-        __syncwarp();
+            for (int s = 0; s < R; s++) {
+                const int k = R * lane + s;
+                sl[k + (k >> 5)] = xs[s];
+            }
+            __syncwarp();
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int k = lane + 32 * r;
-            if (k < nk) x[c0 + k] = sl[k + r];
+            for (int r = 0; r < R; r++) {
+                const int k = lane + 32 * r;
+                if (k < nk) x[c0 + k] = sl[k + r];
+            }
         }
     }
 }
@@ -336,12 +406,29 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const Kry
 // longest line the warp solver takes (32 rows per register slot)
 constexpr int ZL_MAX_R = 8;
 
+// the VEC path's conditions: full 32 R columns, R a power of two up to 8,
+// every row start (k = 0) and stride a multiple of 8 elements, and 16-byte
+// aligned arrays
+bool zline_vec_ok(const ZlineArgs &a, int R) {
+    const MgLevel &v = a.L;
+    auto al = [](const void *p) { return ((uintptr_t)p & 15) == 0; };
+    bool ok = v.n[2] == 32 * R && (R == 1 || R == 2 || R == 4 || R == 8) &&
+              v.at(0, 0, 0) % 8 == 0 && v.g.sx % 8 == 0 && v.g.sy % 8 == 0 && al(a.x) &&
+              al(a.f) && al(v.w[2]);
+    return ok;
+}
+
 template <int R>
 void zline_launch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st, int blocks) {
-    if (a.L.ltab)
-        k_mg_smooth<R, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+    const bool vec = zline_vec_ok(a, R);
+    if (a.L.ltab && vec)
+        k_mg_smooth<R, true, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+    else if (a.L.ltab)
+        k_mg_smooth<R, true, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+    else if (vec)
+        k_mg_smooth<R, false, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
     else
-        k_mg_smooth<R, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+        k_mg_smooth<R, false, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
 }
 
 void zline_dispatch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st) {
