@@ -184,6 +184,15 @@ int mgx_vcycle(void *ctx, const float *f, float *x) {
     return 0;
 }
 
+// Storage facts of level l: {at(0, 0, 0), sx, sy} (the smoother's vector
+// path needs all three to be multiples of 8 elements).
+void mgx_layout(void *ctx, int l, long long *out) {
+    const MgLevel &v = ((HostMg *)ctx)->L[l];
+    out[0] = v.at(0, 0, 0);
+    out[1] = v.g.sx;
+    out[2] = v.g.sy;
+}
+
 // The level's FP32 arrays as the device holds them (cf: n + 1, w: n).
 void mgx_level_arrays(void *ctx, int l, int a, float *cf, float *w) {
     HostMg *m = (HostMg *)ctx;

@@ -44,6 +44,7 @@ def harness():
     lib.mgx_vcycle.argtypes = [C.c_void_p, PF, PF]
     PI = C.POINTER(C.c_int)
     lib.mgx_vcycle_folded.argtypes = [C.c_void_p, PF, PF]
+    lib.mgx_layout.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_longlong)]
     lib.mgx_level_arrays.argtypes = [C.c_void_p, C.c_int, C.c_int, PF, PF]
     lib.mgx_line_table.argtypes = [C.c_void_p, C.c_int, PI, PI, PI, PF]
     return lib
@@ -332,5 +333,24 @@ def test_folded_vcycle_equals_the_plain_one(n):
         Mu, Mv = mg.vcycle_folded(u), mg.vcycle_folded(v)
         assert abs(np.sum(u * Mv) - np.sum(Mu * v)) <= 1e-4 * np.sqrt(np.sum(u * Mu) * np.sum(v * Mv))
         assert np.sum(u * Mu) > 0 and np.sum(v * Mv) > 0
+    finally:
+        mg.close()
+
+
+@pytest.mark.parametrize("n", [(40, 20, 20), (64, 32, 128), (48, 20, 72)])
+def test_rows_start_on_32_byte_boundaries(n):
+    """The smoother's vector path loads each lane's rows with float2/float4
+    accesses: it relies on every level's row start (k = 0 of an interior
+    row) and both strides being multiples of 8 elements, which the storage
+    layout (Grid::make: guide cells shifted so that k = 0 is aligned, rows
+    padded to 8) gives on every level."""
+    cg = casegen()
+    mesh = cg.make_mesh(*n)
+    mg = HostMg(mesh.x, mesh.y, mesh.z, mesh.gc)
+    try:
+        out = (C.c_longlong * 3)()
+        for l in range(len(mg.levels)):
+            mg.lib.mgx_layout(mg.h, l, out)
+            assert out[0] % 8 == 0 and out[1] % 8 == 0 and out[2] % 8 == 0, (l, list(out))
     finally:
         mg.close()
