@@ -23,7 +23,8 @@
 // restriction sums the children's residuals (K is in integrated form), the
 // prolongation copies the coarse correction.  The smoother solves every
 // z-column exactly (zebra Gauss-Seidel over columns coloured (i + j) % 2),
-// colour 0 then 1 before the coarse correction and 1 then 0 after, and the
+// colour 0 then 1 before the coarse correction and 1 then 0 after, mg_nu
+// (level) times each, and the
 // coarsest level is solved exactly with its precomputed inverse: the
 // V-cycle is a symmetric positive definite linear operator, as conjugate
 // gradients require of a preconditioner.
