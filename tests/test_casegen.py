@@ -69,3 +69,25 @@ def test_polar_and_profile():
     assert math.isclose(prof[4, k, 0], (0.05 / 0.41) * math.log(mesh.z[k] / 1e-3))
     U = cg.initial_velocity(spec, mesh)
     assert np.all(U[0] == prof[None, :, :, :][0])    # guide cells untouched by the noise
+
+
+def test_command_line_time_step(tmp_path):
+    """`python -m 3dalm_b200.casegen <config> <dir> --dt` sets the case's
+    time step (the benchmark's 5e-4 on the 512x256x128 configuration) and
+    runtime.time = steps * dt."""
+    cg = casegen()
+    d = str(tmp_path / "case")
+    cg.main(["tiny-loglaw", d, "--dt", "5e-4", "--steps", "3", "--no-state"])
+    setup = json.load(open(f"{d}/setup.json"))
+    text = json.dumps(setup)
+    assert '"dt": 0.0005' in text
+    assert math.isclose(setup["runtime"]["time"], 3 * 5e-4)
+
+
+def test_timeline_kernel_names():
+    import importlib
+    tl = importlib.import_module("3dalm_b200.timeline")
+    assert tl.kernel_name("void dalm::(anonymous namespace)::k_mg_smooth<4, true, true>(x)") \
+        == "k_mg_smooth"
+    assert tl.kernel_name("void dalm::(anonymous namespace)::k_stencil<3>(a)") == "k_stencil<3>"
+    assert tl.kernel_name("k_project(dalm::StepParams)") == "k_project"
