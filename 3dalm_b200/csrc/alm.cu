@@ -1,154 +1,40 @@
 // Actuator-line kernels (FP64), compiled with --fmad=false so the blade-point
 // arithmetic keeps the reference's rounding; only the libm calls (sin, cos,
 // atan, exp) may differ from the host's by an ulp.
-#include "alm.cuh"
+#include "alm_point.cuh"
 
 namespace dalm {
 
 namespace {
 
-constexpr double PI_D = 3.14159265358979323846;  // M_PI (src/type.h:12)
-
 __device__ __forceinline__ double sq(double v) { return v * v; }
-__device__ __forceinline__ double sgn(double v) { return (double)((v > 0.) - (v < 0.)); }
 
-// find_floor_index (src/util.h:119-146)
-__device__ int floor_index(const double *a, double v, int n) {
-    if (v < a[0]) return -1;
-    if (v >= a[n - 1]) return n - 1;
-    int lo = 0, hi = n - 1, found = -1;
-    while (lo <= hi) {
-        int mid = lo + (hi - lo) / 2;
-        if (a[mid] <= v) {
-            found = mid;
-            lo = mid + 1;
-        } else {
-            hi = mid - 1;
-        }
-    }
-    return found;
-}
-
-// frame_transform (src/euler_angle.h:34-62)
-__device__ void frame_transform(const double in[3], double out[3], double angle, int type) {
-    double c = cos(angle), s = sin(angle);
-    double x = in[0], y = in[1], z = in[2];
-    switch (type) {
-    case EULER_ROLL: out[0] = x; out[1] = c * y + s * z; out[2] = -s * y + c * z; break;
-    case EULER_PITCH: out[0] = c * x - s * z; out[1] = y; out[2] = -s * x + c * z; break;
-    case EULER_YAW: out[0] = c * x + s * y; out[1] = -s * x + c * y; out[2] = z; break;
-    default: out[0] = x; out[1] = y; out[2] = z; break;
-    }
-}
-
-// frame_transform_U (src/euler_angle.h:64-127), reproducing its two typos
-// (roll: -s*v + v*w; yaw: ow*(-c*s - s*y)).
-__device__ void frame_transform_U(const double p[3], const double U[3], double out[3],
-                                  double angle, double ow, int type) {
-    double c = cos(angle), s = sin(angle);
-    double x = p[0], y = p[1], z = p[2], u = U[0], v = U[1], w = U[2];
-    switch (type) {
-    case EULER_ROLL:
-        out[0] = 0. + u;
-        out[1] = ow * (-s * y + c * z) + (c * v + s * w);
-        out[2] = ow * (-c * y - s * z) + (-s * v + v * w);
-        break;
-    case EULER_PITCH:
-        out[0] = ow * (-s * x - c * z) + (c * u - s * w);
-        out[1] = 0. + v;
-        out[2] = ow * (c * x - s * z) + (s * u + c * w);
-        break;
-    case EULER_YAW:
-        out[0] = ow * (-s * x + c * y) + (c * u + s * v);
-        out[1] = ow * (-c * s - s * y) + (-s * u + c * v);
-        out[2] = 0. + w;
-        break;
-    default: out[0] = u; out[1] = v; out[2] = w; break;
-    }
-}
-
-__device__ double lin_interp(double v0, double v1, double x0, double x1, double xp) {
-    double fx = (xp - x0) / (x1 - x0);  // src/util.h:166-174
-    return v0 * (1 - fx) + v1 * fx;
-}
-
+// update_ap_position + calc_ap_force (src/alm.h:233-370), one thread per
+// blade point; the arithmetic is almpt's (alm_point.cuh), shared with the
+// host path of the reference-order mode.
 __global__ void k_alm_points(StepParams P, AlmDev A, double t, Vec3<const double> U) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= A.ap_count) return;
-    const Grid &g = P.g;
     const TurbineDev &wt = A.wt[a / A.ap_per_wt];
-    // wt.angle, wt.ow (src/alm.h:236-244)
-    double angle = wt.formula[0] * sin(wt.formula[1] * t + wt.formula[2]) + wt.formula[3];
-    double ow = wt.formula[0] * wt.formula[1] * cos(wt.formula[1] * t + wt.formula[2]);
-    // blade-point position (src/alm.h:250-266)
     int bid = (a % A.ap_per_wt) / A.ap_per_blade;
-    double r = A.r[a];
-    double theta = bid * (2 * PI_D / A.blades) + t * wt.rot_speed;
-    double loc[3] = {wt.rot_center[0], wt.rot_center[1] + r * cos(theta),
-                     wt.rot_center[2] + r * sin(theta)};
-    double xyz[3];
-    frame_transform(loc, xyz, -angle, wt.type);
-    for (int m = 0; m < 3; m++) xyz[m] += wt.base[m];
-    // force (src/alm.h:287-370)
-    int i = floor_index(P.m.x, xyz[0], g.nx);
-    int j = floor_index(P.m.y, xyz[1], g.ny);
-    int k = floor_index(P.m.z, xyz[2], g.nz);
-    double f[3] = {0, 0, 0}, torque = 0, thrust = 0;
-    if (i >= g.gc && i < g.nx - g.gc && j >= g.gc && j < g.ny - g.gc && k >= g.gc &&
-        k < g.nz - g.gc) {
-        long long id[8] = {g.at(i, j, k),         g.at(i + 1, j, k),
-                           g.at(i, j + 1, k),     g.at(i + 1, j + 1, k),
-                           g.at(i, j, k + 1),     g.at(i + 1, j, k + 1),
-                           g.at(i, j + 1, k + 1), g.at(i + 1, j + 1, k + 1)};
-        double x0 = P.m.x[i], x1 = P.m.x[i + 1], y0 = P.m.y[j], y1 = P.m.y[j + 1];
-        double z0 = P.m.z[k], z1 = P.m.z[k + 1];
-        double fx = (xyz[0] - x0) / (x1 - x0), fy = (xyz[1] - y0) / (y1 - y0),
-               fz = (xyz[2] - z0) / (z1 - z0);
+    almpt::Pose q;
+    almpt::point_pose(wt, A.r[a], bid, A.blades, t, q);
+    long long id[8];
+    double frac[3], f[3] = {0, 0, 0}, torque = 0, thrust = 0;
+    if (almpt::point_cell(P.g, P.m.x, P.m.y, P.m.z, q.xyz, id, frac)) {
         double Uap[3];
         for (int m = 0; m < 3; m++) {
             const double *v = U.c[m];
-            // trilinear_interpolate (src/util.h:176-199)
-            double v01 = v[id[0]] * (1 - fx) + v[id[1]] * fx;
-            double v23 = v[id[2]] * (1 - fx) + v[id[3]] * fx;
-            double v45 = v[id[4]] * (1 - fx) + v[id[5]] * fx;
-            double v67 = v[id[6]] * (1 - fx) + v[id[7]] * fx;
-            double v0123 = v01 * (1 - fy) + v23 * fy;
-            double v4567 = v45 * (1 - fy) + v67 * fy;
-            Uap[m] = v0123 * (1 - fz) + v4567 * fz;
+            double c8[8];
+            for (int n = 0; n < 8; n++) c8[n] = v[id[n]];
+            Uap[m] = almpt::trilinear(c8, frac);
         }
-        double rel[3] = {xyz[0] - wt.base[0], xyz[1] - wt.base[1], xyz[2] - wt.base[2]};
-        double Ur[3];
-        frame_transform_U(rel, Uap, Ur, angle, ow, wt.type);
-        double ux_ = Ur[0];
-        double ut_ = r * wt.rot_speed + Ur[1] * sin(theta) - Ur[2] * cos(theta);
-        double urel2 = ux_ * ux_ + ut_ * ut_;
-        double phi = atan(ux_ / ut_);
-        double atk = phi * 180 / PI_D - A.twist[a];
-        // lookup_cdcl_table (src/alm.h:208-231)
-        const double *cdt = A.cd + (long long)a * A.atk_count;
-        const double *clt = A.cl + (long long)a * A.atk_count;
-        int ti = floor_index(A.atk, atk, A.atk_count);
-        double cd, cl;
-        if (ti < 0) {
-            cd = cdt[0]; cl = clt[0];
-        } else if (ti >= A.atk_count - 1) {
-            cd = cdt[A.atk_count - 1]; cl = clt[A.atk_count - 1];
-        } else {
-            cd = lin_interp(cdt[ti], cdt[ti + 1], A.atk[ti], A.atk[ti + 1], atk);
-            cl = lin_interp(clt[ti], clt[ti + 1], A.atk[ti], A.atk[ti + 1], atk);
-        }
-        double fd = 0.5 * cd * urel2 * A.chord[a] * A.dr[a];
-        double fl = 0.5 * cl * urel2 * A.chord[a] * A.dr[a];
-        double fx_ = fl * cos(phi) + fd * sin(phi);
-        double ft_ = fl * sin(phi) - fd * cos(phi);
-        ft_ *= sgn(wt.rot_speed);
-        double f_[3] = {-fx_, ft_ * sin(theta), -ft_ * cos(theta)};
-        frame_transform(f_, f, -angle, wt.type);
-        torque = fabs(ft_) * r;
-        thrust = fx_;
+        almpt::point_force(wt, q, Uap, A.twist[a], A.chord[a], A.dr[a], A.atk, A.atk_count,
+                           A.cd + (long long)a * A.atk_count, A.cl + (long long)a * A.atk_count,
+                           f, torque, thrust);
     }
     for (int m = 0; m < 3; m++) {
-        A.pt_xyz[a * 3 + m] = xyz[m];
+        A.pt_xyz[a * 3 + m] = q.xyz[m];
         A.pt_f[a * 3 + m] = f[m];
     }
     A.pt_torque[a] = torque;

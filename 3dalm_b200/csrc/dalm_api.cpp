@@ -15,11 +15,12 @@
 #include <fstream>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/dalm.h"
 #include "adjoint.cuh"
-#include "alm.cuh"
+#include "alm_point.cuh"
 #include "case_io.hpp"
 #include "multigrid.cuh"
 #include "multigrid_setup.hpp"
@@ -136,6 +137,10 @@ struct dalm_handle {
     Box fbox{{0, 0, 0}, {0, 0, 0}};
     std::vector<double> pitch_deg;  // collective pitch per turbine (dalm_set_turbine_params)
     double last_alm_time = 0;       // time of the last actuator-line evaluation
+    // reference-order mode: blade points evaluated on the host (alm_points_host)
+    long long *d_alm_ids = nullptr;  // [ap][8] stored indices of the sampling corners
+    double *d_alm_corner = nullptr;  // [ap][8][3] velocity at those corners
+    std::vector<double> h_pt_xyz, h_pt_f;  // [ap][3] positions and forces of the last evaluation
     // runtime
     int64_t step = 0, tavg_count = 0, last_it = 0;
     int64_t max_it = 0;
@@ -869,15 +874,141 @@ struct dalm_handle {
         return u;
     }
 
+    // The blade-point model (update_ap_position + calc_ap_force,
+    // src/alm.h:233-414) on the host, for the reference-order mode: the
+    // same almpt functions as k_alm_points, with the host's libm sin, cos
+    // and atan (the reference's), so positions, angles and loads are the
+    // reference's bit for bit.  The velocity at the 8 sampling corners of
+    // every point is gathered on the device and read back (one synchronising
+    // round trip per evaluation); the results go to the device arrays the
+    // projection and the statistics read.
+    void alm_points_host(double tm, Vec3<const double> u) {
+        const int n = alm.ap_count;
+        if (!d_alm_ids) {
+            d_alm_ids = dalloc<long long>(8 * (size_t)n);
+            d_alm_corner = dalloc<double>(24 * (size_t)n);
+        }
+        std::vector<almpt::Pose> pose((size_t)n);
+        std::vector<long long> ids(8 * (size_t)n, g.at(g.gc, g.gc, g.gc));
+        std::vector<double> frac(3 * (size_t)n, 0.0);
+        std::vector<char> inside((size_t)n, 0);
+        for (int a = 0; a < n; a++) {
+            const TurbineDev &wt = h_wt[a / alm.ap_per_wt];
+            int bid = (a % alm.ap_per_wt) / alm.ap_per_blade;
+            almpt::point_pose(wt, cs.ap_r[a], bid, alm.blades, tm, pose[a]);
+            inside[a] = almpt::point_cell(g, cs.x.data(), cs.y.data(), cs.z.data(), pose[a].xyz,
+                                          &ids[8 * (size_t)a], &frac[3 * (size_t)a]);
+        }
+        DALM_CUDA(cudaMemcpyAsync(d_alm_ids, ids.data(), sizeof(long long) * ids.size(),
+                                  cudaMemcpyHostToDevice, stream));
+        launch_gather_points(L, u, d_alm_ids, 8 * n, d_alm_corner);
+        std::vector<double> corner(24 * (size_t)n);
+        DALM_CUDA(cudaMemcpyAsync(corner.data(), d_alm_corner, sizeof(double) * corner.size(),
+                                  cudaMemcpyDeviceToHost, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        std::vector<double> &xyz = h_pt_xyz, &f = h_pt_f;
+        xyz.assign(3 * (size_t)n, 0.0);
+        f.assign(3 * (size_t)n, 0.0);
+        std::vector<double> tq((size_t)n, 0.0), th((size_t)n, 0.0), sums(2 * (size_t)alm.wt_count, 0.0);
+        const int na = alm.atk_count;
+        for (int a = 0; a < n; a++) {
+            for (int m = 0; m < 3; m++) xyz[3 * (size_t)a + m] = pose[a].xyz[m];
+            if (!inside[a]) continue;
+            double Uap[3];
+            for (int m = 0; m < 3; m++) {
+                double c8[8];
+                for (int q = 0; q < 8; q++) c8[q] = corner[(8 * (size_t)a + q) * 3 + m];
+                Uap[m] = almpt::trilinear(c8, &frac[3 * (size_t)a]);
+            }
+            almpt::point_force(h_wt[a / alm.ap_per_wt], pose[a], Uap, twist[a], cs.ap_chord[a],
+                               cs.ap_dr[a], cs.atk.data(), na, &cs.ap_cd[(size_t)a * na],
+                               &cs.ap_cl[(size_t)a * na], &f[3 * (size_t)a], tq[a], th[a]);
+        }
+        // per-turbine sums in blade-point order (src/alm.h:384-398)
+        for (int w = 0; w < alm.wt_count; w++) {
+            double torque = 0, thrust = 0;
+            for (int a = w * alm.ap_per_wt; a < (w + 1) * alm.ap_per_wt; a++) {
+                torque += tq[a];
+                thrust += th[a];
+            }
+            sums[w] = torque;
+            sums[alm.wt_count + w] = thrust;
+        }
+        const size_t b3 = sizeof(double) * 3 * (size_t)n, b1 = sizeof(double) * (size_t)n,
+                     bw = sizeof(double) * (size_t)alm.wt_count;
+        DALM_CUDA(cudaMemcpyAsync(alm.pt_xyz, xyz.data(), b3, cudaMemcpyHostToDevice, stream));
+        DALM_CUDA(cudaMemcpyAsync(alm.pt_f, f.data(), b3, cudaMemcpyHostToDevice, stream));
+        DALM_CUDA(cudaMemcpyAsync(alm.pt_torque, tq.data(), b1, cudaMemcpyHostToDevice, stream));
+        DALM_CUDA(cudaMemcpyAsync(alm.pt_thrust, th.data(), b1, cudaMemcpyHostToDevice, stream));
+        DALM_CUDA(cudaMemcpyAsync(alm.wt_torque, sums.data(), bw, cudaMemcpyHostToDevice, stream));
+        DALM_CUDA(cudaMemcpyAsync(alm.wt_thrust, sums.data() + alm.wt_count, bw,
+                                  cudaMemcpyHostToDevice, stream));
+        // the host vectors go out of scope at return: wait for the copies
+        DALM_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // distribute_ap_force (src/alm.h:416-448) on the host for the
+    // reference-order mode: every interior cell sums every blade point in
+    // point order with the host's exp, untruncated, exactly the reference's
+    // loop; the whole field is uploaded and the predictor reads it on the
+    // whole interior.  Cells are independent, so host threads split the
+    // i-planes without changing any result.
+    void alm_project_host() {
+        const int n = alm.ap_count, gc = (int)cs.gc;
+        const double pw = cs.projection_width;
+        const double c = pw * sqrt(PI_D);
+        const double e = 1 / (c * c * c);  // 1/cubic(projection_width*sqrt(Pi))
+        std::vector<double> fh[3];
+        for (auto &v : fh) v.assign((size_t)g.total, 0.0);
+        auto planes = [&](int i0, int i1) {
+            for (int i = i0; i < i1; i++)
+                for (int j = gc; j < g.ny - gc; j++)
+                    for (int k = gc; k < g.nz - gc; k++) {
+                        double fx = 0, fy = 0, fz = 0;
+                        const double xc = cs.x[i], yc = cs.y[j], zc = cs.z[k];
+                        for (int a = 0; a < n; a++) {
+                            const double *p = &h_pt_xyz[3 * (size_t)a];
+                            const double dx = xc - p[0], dy = yc - p[1], dz = zc - p[2];
+                            const double r2 = dx * dx + dy * dy + dz * dz;
+                            const double wght = e * exp(-r2 / (pw * pw));
+                            fx += wght * h_pt_f[3 * (size_t)a];
+                            fy += wght * h_pt_f[3 * (size_t)a + 1];
+                            fz += wght * h_pt_f[3 * (size_t)a + 2];
+                        }
+                        const long long id = g.at(i, j, k);
+                        fh[0][id] = fx;
+                        fh[1][id] = fy;
+                        fh[2][id] = fz;
+                    }
+        };
+        const int ni = g.nx - 2 * gc;
+        int nt = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), 32u);
+        nt = std::max(1, std::min(nt, ni));
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; t++)
+            pool.emplace_back(planes, gc + (int)((long long)ni * t / nt), gc + (int)((long long)ni * (t + 1) / nt));
+        for (auto &th : pool) th.join();
+        for (int m = 0; m < 3; m++)
+            DALM_CUDA(cudaMemcpyAsync(F[m], fh[m].data(), sizeof(double) * (size_t)g.total,
+                                      cudaMemcpyHostToDevice, stream));
+        DALM_CUDA(cudaStreamSynchronize(stream));
+        fbox = Box{{gc, gc, gc}, {g.nx - gc, g.ny - gc, g.nz - gc}};
+    }
+
     void stage_alm() { alm_at(cs.dt * (double)step); }  // rt.get_time(), src/solver.h:189-191
     void alm_at(double tm) {
         if (alm.ap_count == 0) return;
         StageTimer t(this, DALM_STAGE_ALM);
         last_alm_time = tm;
-        launch_alm_points(L, P, alm, tm, c(u_cur()));
-        Box cur = force_box(tm);
-        launch_alm_project(L, P, alm, unite(fbox, cur), f3());
-        fbox = cur;
+        if (opt.reference_sums) {
+            alm_points_host(tm, c(u_cur()));
+            alm_project_host();
+        } else {
+            launch_alm_points(L, P, alm, tm, c(u_cur()));
+            Box cur = force_box(tm);
+            launch_alm_project(L, P, alm, unite(fbox, cur), f3());
+            fbox = cur;
+        }
         DALM_CUDA(cudaMemcpyAsync(h_wt_out, alm.wt_torque, sizeof(double) * alm.wt_count,
                                   cudaMemcpyDeviceToHost, stream));
         DALM_CUDA(cudaMemcpyAsync(h_wt_out + alm.wt_count, alm.wt_thrust, sizeof(double) * alm.wt_count,

@@ -5,14 +5,14 @@ Two modes of the same kernels:
 
   reference_sums=True   every global sum (Krylov dots, residual and
                         divergence norms) is accumulated in the reference's
-                        serial cell order.  Every other operation already keeps
+                        serial cell order, and the actuator line (blade-point
+                        model and Gaussian projection) runs on the host with
+                        the host's libm.  Every other operation already keeps
                         the reference's order and rounding (FP64, no FMA
-                        contraction, host-libm Smagorinsky filter), so without
-                        turbines the GPU step must be BIT-IDENTICAL to the
-                        reference: fields, Poisson iteration counts, residuals.
-                        With turbines the device libm (sin, cos, atan, exp) may
-                        differ from the host's by an ulp in the blade-point
-                        forces, so those cases use the envelope below.
+                        contraction, host-libm Smagorinsky filter), so the GPU
+                        step must be BIT-IDENTICAL to the reference: fields,
+                        Poisson iteration counts, residuals, blade-point
+                        positions, forces and turbine loads.
   default (fast)        the sums use a deterministic parallel tree.  The
                         reference algorithm itself moves by the envelope
                         ENVELOPE under a change of summation order alone
@@ -139,33 +139,63 @@ def test_fast_mode_10_steps_within_envelope(make_case, name):
 
 
 @pytest.mark.parametrize("name", TURBINE)
-def test_reference_sums_turbines_10_steps(make_case, name):
+def test_reference_sums_turbines_bit_identical_10_steps(make_case, name):
+    """With reference-order sums the blade-point model and the Gaussian
+    projection run on the host with the host's libm (the reference's), so
+    turbine cases are bit-identical too: fields, iteration counts, residuals,
+    blade-point positions, forces and turbine loads at every step."""
     s, o = setup_pair(make_case, name, reference_sums=True)
-    first_diff = None
+    assert_points_identical(s, o, "set_state")
+    assert_identical(s, o, ("U", "JU", "f", "nut", "div"), "set_state")
     for n in range(11):
         s.step(1)
         o.step(1)
-        within_envelope(s, o, n, "reference-sums")
-        if first_diff is None and s.stats()["it"] != o.stats()["it"]:
-            first_diff = n
-    # the blade-point loads themselves match to libm-ulp level
+        ss, so = s.stats(), o.stats()
+        assert ss["it"] == so["it"], f"step {n}: iterations {ss['it']} != {so['it']}"
+        assert ss["err"] == so["err"] and ss["avg_div"] == so["avg_div"], f"step {n}"
+        assert ss["max_cfl"] == so["max_cfl"], f"step {n}"
+        assert_identical(s, o, ("U", "p", "f"), f"step {n}")
+        assert_points_identical(s, o, f"step {n}")
+    assert_identical(s, o, ("JU", "nut", "div", "b", "Uold"), "after 10 steps")
+
+
+def assert_points_identical(s, o, where):
+    xs, fs, tqs, ths = s.points()
+    xo, fo, tqo, tho = o.points()
+    np.testing.assert_array_equal(xs, xo, err_msg=f"{where}: blade-point positions")
+    np.testing.assert_array_equal(fs, fo, err_msg=f"{where}: blade-point forces")
+    np.testing.assert_array_equal(tqs, tqo, err_msg=f"{where}: blade-point torque")
+    np.testing.assert_array_equal(ths, tho, err_msg=f"{where}: blade-point thrust")
+    th, tq, _ = s.turbines()
+    tqo_w, tho_w = o.turbines()
+    np.testing.assert_array_equal(th, tho_w, err_msg=f"{where}: turbine thrust")
+    np.testing.assert_array_equal(tq, tqo_w, err_msg=f"{where}: turbine torque")
+
+
+@pytest.mark.parametrize("name", TURBINE)
+def test_fast_mode_blade_points(make_case, name):
+    """The fast mode evaluates the blade points on the device (device sin,
+    cos, atan) and projects with the device exp, truncated at r^2 <= 40 eps^2:
+    positions within 1e-13 absolute, forces and the force field within
+    1e-12 relative of the oracle's on the same velocity."""
+    s, o = setup_pair(make_case, name)
     xs, fs, _, _ = s.points()
     xo, fo, _, _ = o.points()
     np.testing.assert_allclose(xs, xo, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(fs, fo, rtol=1e-12, atol=1e-16)
+    assert_close(s, o, ("f",), 1e-12, "set_state")
 
 
 def test_turbine_params_and_points(make_case):
     params = ([12.0], [3.0], [9.0])
     s, o = setup_pair(make_case, "tiny-turbine", params=params, reference_sums=True)
+    assert_points_identical(s, o, "set_state")
     s.step(1)
     o.step(1)
-    xs, fs, tqs, ths = s.points()
-    xo, fo, tqo, tho = o.points()
-    np.testing.assert_allclose(xs, xo, rtol=0, atol=1e-13)
-    np.testing.assert_allclose(fs, fo, rtol=1e-12, atol=1e-16)
+    assert_points_identical(s, o, "step 1")
     th, tq, pw = s.turbines()
     np.testing.assert_allclose(pw, tq * 9.0, rtol=1e-15)
-    assert_close(s, o, ("f",), 1e-12, "params")
+    assert_identical(s, o, ("f", "U", "p"), "params")
 
 
 def test_field_round_trip(make_case):
