@@ -42,7 +42,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s"
 CASE = "c4"
-SAMPLE_N = (256, 128, 64)  # interior cells of the CPU baseline's sample
 # Time step of the benchmark runs.  At the configured dt = 1e-3 the
 # 512x256x128 case diverges in the reference's explicit scheme (both forms
 # here, the FP64 one step for step like the reference): the per-cell 8 %
@@ -52,24 +51,6 @@ SAMPLE_N = (256, 128, 64)  # interior cells of the CPU baseline's sample
 # over steps 1-5).  At dt = 5e-4 every setting else as configured runs
 # stably (max CFL 0.08 falling to 0.02 over 60 steps).
 BENCH_DT = 5e-4
-
-# BiCGStab iterations of each time step of this workload (seed 0, dt =
-# BENCH_DT, step 0 has no pressure solve), measured by this benchmark's GPU
-# arm in its default fast mode (None: not measured).  The reference's counts
-# on the same steps differ only by the summation-order spread
-# (tests/test_oracle_sensitivity.py), so the reference arm times its CPU
-# code per iteration and per cell and models the steps the GPU arm times
-# (steps W .. W+K-1) with these counts.
-C4_ITERATIONS = [0, None, None, 366, 111, 331, 218]
-
-
-def step_iterations(warmup, steps):
-    """Mean iteration count of the timed steps warmup .. warmup+steps-1, or
-    None when they lie beyond the measured list."""
-    sel = C4_ITERATIONS[warmup:warmup + steps]
-    ok = len(sel) == steps and steps > 0 and all(v is not None for v in sel)
-    return statistics.mean(sel) if ok else None
-
 
 def workload_config(case, cells, iterations, world, dt=BENCH_DT):
     """The `config` object both arms report."""
@@ -242,79 +223,111 @@ def make_case(name, tmp, dt=BENCH_DT):
 
 # ------------------------------------------------------------------ CPU side
 
-def cpu_sample(kind_pref="reference", iterations=None, poisson_cap=40):
-    """Time the CPU oracle (the reference compiled from its own sources when
-    available, else the C restatement) stage by stage on a bounded sample:
-    the same 3-turbine case at 256x128x64 cells (2,097,152; 17 MB per field,
-    beyond one core's caches), one integrating step with the Poisson solve
-    capped at `poisson_cap` iterations.  The
-    per-cell stage costs, the per-cell-per-iteration Poisson cost and the
-    per-cell-per-blade-point projection cost are combined into the time of
-    one full 512x256x128 step with `iterations` Poisson iterations (serial,
-    one core).  Returns (Mcell-steps/s, kind, description)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+REF_MPIRUN = os.path.join(ROOT, "oracle", "_ref", "ref_mpirun")
 
-    kind = "reference" if (kind_pref == "reference" and O.reference_available()) else "port"
-    if kind == "port" and not os.path.exists(O.LIB_C):
-        O.build()
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# Wall budget of the reference arm: no timed reference step begins after
+# this many seconds since the start (every step that runs is whole and
+# uncapped; the line says how many ran).  On the 16-core GPU hosts a whole
+# step of the 512x256x128 case takes ~0.15-0.25 s per BiCGStab iteration, and
+# the warm-up steps from the seeded state take ~3000 iterations.
+REF_BUDGET_S = float(os.environ.get("DALM_REF_BUDGET_S", "900"))
+
+
+def run_reference_ranks(case, warmup, steps, ranks, max_it=None, budget=0.0, timeout=3000):
+    """The reference's own time step (oracle/_ref/ref_mpirun: the reference
+    compiled from its sources, OpenACC off, with a shared-memory MPI subset)
+    as `ranks` MPI ranks on the host cores: the 3-turbine case from its seeded
+    initial state, `warmup` untimed steps, then `steps` timed whole steps.
+    Returns ref_mpirun's result (per-step seconds, Poisson iterations and
+    residuals) plus the case's description."""
     cg = importlib.import_module("3dalm_b200.casegen")
-    full = cg.config(CASE)
-    spec = cg.config(CASE, n=SAMPLE_N, steps=10)
-    with tempfile.TemporaryDirectory() as d, quiet_stdout():
+    over = {"steps": 100000, "dt": BENCH_DT}
+    if max_it:
+        over["max_it"] = max_it
+    spec = cg.config(case, **over)
+    with tempfile.TemporaryDirectory(prefix="dalm_ref_") as d, quiet_stdout():
         mesh = cg.write_case(spec, d)
-        o = O.Reference(d) if kind == "reference" else O.CRestatement(d)
-        prof = cg.inflow_profile(spec, mesh)
-        o.set_inflow_profile(prof)
-        o.set_state(cg.initial_velocity(spec, mesh))
-        o.advance_clock()
-        o.set_poisson(poisson_cap, 0.0)
-        t = []
-        for st in range(6):
-            t0 = time.perf_counter()
-            o.stage(st)
-            t.append(time.perf_counter() - t0)
-        it = o.stats()["it"]
-        n_pts = o.turbine_count() * 3 * spec.points_per_blade
-        o.close()
-    n_s = spec.n[0] * spec.n[1] * spec.n[2]
-    n_f = full.n[0] * full.n[1] * full.n[2]
-    per_cell = (t[0] + t[1] + t[3] + t[5]) / n_s
-    per_iter = t[2] / (it * n_s)
-    per_cell_point = t[4] / (n_s * n_pts)
-    its = iterations if iterations else it
-    step_time = n_f * (per_cell + its * per_iter) + n_f * n_pts * per_cell_point
-    desc = (f"{'reference (oracle/_ref)' if kind == 'reference' else 'C restatement'} serial, "
-            f"stage-timed on the same case at {'x'.join(map(str, SAMPLE_N))} ({n_s} cells, "
-            f"{n_pts} blade points, "
-            f"Poisson capped at {it} iterations); per-cell, per-cell-iteration and "
-            f"per-cell-point costs scaled to 512x256x128 with {its:.1f} Poisson iterations/step")
-    return n_f / step_time / 1e6, kind, desc, sum(t)
+        cg.write_state_files(spec, mesh, d)
+        out = os.path.join(d, "result.json")
+        cmd = [REF_MPIRUN, d, "--ranks", str(ranks), "--warmup", str(warmup), "--steps", str(steps),
+               "--out", out, "--state", os.path.join(d, cg.STATE_FILE), "--budget", str(budget)]
+        prof = os.path.join(d, cg.PROFILE_FILE)
+        if os.path.exists(prof):
+            cmd += ["--profile", prof]
+        w0 = time.perf_counter()
+        r = subprocess.run(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True,
+                           timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_mpirun failed ({r.returncode}): {r.stderr[-2000:]}")
+        with open(out) as f:
+            res = json.load(f)
+        res["wall_seconds"] = time.perf_counter() - w0
+    return res
+
+
+def reference_sample(ranks, iterations):
+    """cpu_baseline: a bounded sample of the benchmark workload on the host
+    cores: one whole step (step 1 from the seeded initial state) of the full
+    512x256x128 case through the reference's own code as `ranks` MPI ranks,
+    with its pressure solve capped at the GPU arm's mean iteration count of
+    the timed steps (so the sample does the same work per step as they do)."""
+    it = max(1, int(round(iterations)))
+    res = run_reference_ranks(CASE, 1, 1, ranks, max_it=it)
+    secs = res["seconds"]
+    desc = (f"reference (oracle/_ref/ref_mpirun: the reference's own step, OpenACC off) as "
+            f"{ranks} MPI ranks on {ranks} host cores; one whole step of the same "
+            f"512x256x128 case (step 1 from the seeded initial state) with the pressure "
+            f"solve capped at {it} iterations, the GPU arm's mean over its timed steps "
+            f"(ran {res['iterations'][0]})")
+    return res["cells"] / secs / 1e6, "reference", desc, secs
 
 
 def run_reference(args):
+    """--impl reference: the reference's own CPU implementation of the step
+    (MPI ranks on every host core, the reference's x-slab decomposition, OpenACC
+    off) on the same case, steps and metric as this benchmark's arm: W untimed
+    warm-up steps from the seeded initial state, then K timed whole steps."""
     rank, world, local = dist_env()
     if rank != 0:
         return
-    iters = step_iterations(args.warmup, args.steps) if args.case == CASE else None
-    vals = []
-    for n in range(args.warmup + args.steps):
-        # warm-up samples only page the code and data in: a short solve
-        v, kind, desc, secs = cpu_sample("reference", iters, 40 if n >= args.warmup else 4)
-        if n >= args.warmup:
-            vals.append(v)
-    value = statistics.mean(vals)
+    if not os.path.exists(REF_MPIRUN):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/ref_mpirun was not built (the reference sources were "
+                          "absent when __graft_entry__.build() ran)"}), flush=True)
+        return
+    ranks = host_cores()
+    res = run_reference_ranks(args.case, args.warmup, args.steps, ranks, budget=REF_BUDGET_S)
+    secs = res["seconds"]
+    cells = res["cells"]
+    timed = res["steps_timed"]
+    value = cells * timed / secs / 1e6
+    desc = (f"reference (oracle/_ref/ref_mpirun: the reference's own step compiled from its "
+            f"sources, OpenACC off, -O3 AVX2/FMA) as {ranks} MPI ranks (x-slabs, shared-memory "
+            f"MPI) on {ranks} host cores; steps {args.warmup}..{args.warmup + timed - 1} "
+            f"of the case after {args.warmup} untimed warm-up steps from the seeded initial "
+            f"state, every step whole (Poisson to its tolerance); {timed} of the {args.steps} "
+            f"requested steps fitted the {REF_BUDGET_S:.0f} s wall budget")
+    cfg = workload_config(args.case, cells, res["iterations"], args.gpus)
+    cfg["reference_residuals"] = res["residuals"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 16777216 / (value * 1e6) * 1e3, "higher_is_better": True,
+        "ms_per_step": secs / timed * 1e3, "steps_timed": timed, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args.case, 16777216,
-                                  C4_ITERATIONS[args.warmup:args.warmup + args.steps], args.gpus),
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": kind,
-                         "sample": desc + "; the reference's CPU path is serial (OpenACC/MPI "
-                                          "code built without either)"},
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": ranks, "kind": "reference",
+                         "sample": desc},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_seconds": res["step_seconds"],
+        "setup_seconds": res["init_seconds"], "warmup_seconds": res["warmup_seconds"],
     }
     print(json.dumps(line), flush=True)
 
@@ -528,9 +541,10 @@ def run_ours(args):
     }
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_cost(pkg, local)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, kind, desc, secs = cpu_sample("reference", statistics.mean(its))
-        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": 1, "kind": kind,
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_MPIRUN):
+        ranks = host_cores()
+        v, kind, desc, secs = reference_sample(ranks, statistics.mean(its))
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": ranks, "kind": kind,
                                 "sample": desc, "sample_seconds": secs}
     s.finalize()
     if rank == 0:

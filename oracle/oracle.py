@@ -52,6 +52,17 @@ def build(ref: bool = False) -> None:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
+def reference_src() -> str:
+    """The reference's source tree (its src/ directory): $DALM_REFERENCE_SRC,
+    else oracle/Makefile's REFERENCE_SRC."""
+    env = os.environ.get("DALM_REFERENCE_SRC")
+    if env:
+        return env
+    r = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "print-reference-src"],
+                       capture_output=True, text=True)
+    return r.stdout.strip()
+
+
 def reference_available() -> bool:
     return os.path.exists(LIB_REF)
 

@@ -15,7 +15,7 @@ import pytest
 from conftest import casegen
 import oracle as O
 
-REF_SRC = "/root/reference"
+REF_SRC = os.path.dirname(O.reference_src().rstrip("/"))  # the reference tree
 
 
 def _have_ref():
