@@ -12,7 +12,10 @@ __device__ __forceinline__ double sq(double v) { return v * v; }
 // update_ap_position + calc_ap_force (src/alm.h:233-370), one thread per
 // blade point; the arithmetic is almpt's (alm_point.cuh), shared with the
 // host path of the reference-order mode.
-__global__ void k_alm_points(StepParams P, AlmDev A, double t, Vec3<const double> U) {
+// T: storage type of the velocity field (double, or float for the mixed
+// form's FP32 stencil fields); the point model is FP64 either way.
+template <typename T>
+__global__ void k_alm_points(StepParams P, AlmDev A, double t, Vec3<const T> U) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= A.ap_count) return;
     const TurbineDev &wt = A.wt[a / A.ap_per_wt];
@@ -24,9 +27,9 @@ __global__ void k_alm_points(StepParams P, AlmDev A, double t, Vec3<const double
     if (almpt::point_cell(P.g, P.m.x, P.m.y, P.m.z, q.xyz, id, frac)) {
         double Uap[3];
         for (int m = 0; m < 3; m++) {
-            const double *v = U.c[m];
+            const T *v = U.c[m];
             double c8[8];
-            for (int n = 0; n < 8; n++) c8[n] = v[id[n]];
+            for (int n = 0; n < 8; n++) c8[n] = (double)v[id[n]];
             Uap[m] = almpt::trilinear(c8, frac);
         }
         almpt::point_force(wt, q, Uap, A.twist[a], A.chord[a], A.dr[a], A.atk, A.atk_count,
@@ -58,8 +61,9 @@ __global__ void k_alm_sums(AlmDev A) {
 // gathers, in blade-point order, the points whose truncated support reaches
 // its tile, then every cell of the tile sums those points in that order
 // (the reference's order with the negligible far terms left out).
+template <typename FT>
 __global__ void __launch_bounds__(TILE_THREADS)
-k_alm_project(StepParams P, AlmDev A, Tiling T, Vec3<double> F) {
+k_alm_project(StepParams P, AlmDev A, Tiling T, Vec3<FT> F) {
     extern __shared__ int list[];
     __shared__ int warp_count[TILE_THREADS / 32];
     __shared__ int total;
@@ -119,9 +123,9 @@ k_alm_project(StepParams P, AlmDev A, Tiling T, Vec3<double> F) {
                 }
             }
             long long c = g.at(i, j, k);
-            F.c[0][c] = fx;
-            F.c[1][c] = fy;
-            F.c[2][c] = fz;
+            F.c[0][c] = (FT)fx;
+            F.c[1][c] = (FT)fy;
+            F.c[2][c] = (FT)fz;
         }
         __syncthreads();
     }
@@ -129,26 +133,36 @@ k_alm_project(StepParams P, AlmDev A, Tiling T, Vec3<double> F) {
 
 }  // namespace
 
+template <typename T>
 void launch_alm_points(const LaunchCtx &L, const StepParams &P, const AlmDev &A, double t,
-                       Vec3<const double> u) {
+                       Vec3<const T> u) {
     if (A.ap_count <= 0) return;
     L.pre(KK_ALM_POINTS);
-    k_alm_points<<<(A.ap_count + 63) / 64, 64, 0, L.s>>>(P, A, t, u);
+    k_alm_points<T><<<(A.ap_count + 63) / 64, 64, 0, L.s>>>(P, A, t, u);
     L.post(KK_ALM_POINTS);
     L.pre(KK_ALM_SUMS);
     k_alm_sums<<<1, 32 * ((A.wt_count + 31) / 32), 0, L.s>>>(A);
     L.post(KK_ALM_SUMS);
 }
+template void launch_alm_points<double>(const LaunchCtx &, const StepParams &, const AlmDev &,
+                                        double, Vec3<const double>);
+template void launch_alm_points<float>(const LaunchCtx &, const StepParams &, const AlmDev &,
+                                       double, Vec3<const float>);
 
+template <typename FT>
 void launch_alm_project(const LaunchCtx &L, const StepParams &P, const AlmDev &A,
-                        const Box &box, Vec3<double> f) {
+                        const Box &box, Vec3<FT> f) {
     if (A.ap_count <= 0 || box.empty()) return;
     Tiling T = Tiling::make(box);
     long long blocks = T.ntiles < 4096 ? T.ntiles : 4096;
     size_t smem = sizeof(int) * (size_t)A.ap_count;
     L.pre(KK_ALM_PROJECT);
-    k_alm_project<<<(int)blocks, TILE_THREADS, smem, L.s>>>(P, A, T, f);
+    k_alm_project<FT><<<(int)blocks, TILE_THREADS, smem, L.s>>>(P, A, T, f);
     L.post(KK_ALM_PROJECT);
 }
+template void launch_alm_project<double>(const LaunchCtx &, const StepParams &, const AlmDev &,
+                                         const Box &, Vec3<double>);
+template void launch_alm_project<float>(const LaunchCtx &, const StepParams &, const AlmDev &,
+                                        const Box &, Vec3<float>);
 
 }  // namespace dalm

@@ -29,11 +29,16 @@ struct AlmDev {
 
 // update_ap_position + calc_ap_force (src/alm.h:233-414) and the per-turbine
 // sums (src/alm.h:384-398).
+// T: storage type of the sampled velocity (double, or float for the mixed
+// form's FP32 stencil fields)
+template <typename T>
 void launch_alm_points(const LaunchCtx &L, const StepParams &P, const AlmDev &A, double t,
-                       Vec3<const double> u);
+                       Vec3<const T> u);
 // distribute_ap_force (src/alm.h:416-448) confined to each point's support,
 // over `box` (cells outside every support get 0).
+// FT: storage type of the force field
+template <typename FT>
 void launch_alm_project(const LaunchCtx &L, const StepParams &P, const AlmDev &A,
-                        const Box &box, Vec3<double> f);
+                        const Box &box, Vec3<FT> f);
 
 }  // namespace dalm

@@ -272,6 +272,12 @@ struct LaunchCtx {
     void (*hook)(void *self, int kind, int phase) = nullptr;  // phase 0 before, 1 after
     void *self = nullptr;
     long long *launches = nullptr;
+    // per-kind algorithmic bytes of the launches, for kernels whose bytes
+    // depend on the launch (multigrid levels); accumulated when profiling
+    double *kind_bytes = nullptr;
+    void bytes(int kind, double b) const {
+        if (kind_bytes) kind_bytes[kind] += b;
+    }
     void pre(int kind) const {
         if (hook) hook(self, kind, 0);
     }

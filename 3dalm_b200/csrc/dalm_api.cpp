@@ -108,7 +108,14 @@ struct dalm_handle {
     bool mg_on = false;
     MgDev mgd;
     MgPcgBufs mgb{};
-    MixedGeom geo{};  // the FP32 predictor's mesh table
+    MixedGeom geo{};  // mesh tables of the FP32 flow stages
+    // DALM_MIXED stencil fields in FP32 (not with reference-order sums): the
+    // stages run on these; U, JU and F above are FP64 views of them,
+    // refreshed (widen) when the ABI reads the state and written back
+    // (narrow) when it sets it.
+    bool f32 = false;
+    bool f64_stale = false;
+    float *U32[2][3] = {}, *JU32[2][3] = {}, *F32[3] = {};
     FusedBufs fb{};
     bool fused = false;  // BiCGStab iterations as fused half-iteration kernels
     PoissonConfig pcfg{};
@@ -151,6 +158,7 @@ struct dalm_handle {
     std::vector<EventPair> ev_pending;
     cudaEvent_t ev_open = nullptr;
     double kind_ms[KK_COUNT] = {};
+    double kind_bytes[KK_COUNT] = {};  // launch-dependent algorithmic bytes (LaunchCtx::bytes)
     int64_t kind_launches[KK_COUNT] = {};
     double stage_ms[7] = {};
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_pending;
@@ -285,6 +293,7 @@ struct dalm_handle {
         if (opt.profile) {
             L.hook = &dalm_handle::hook;
             L.self = this;
+            L.kind_bytes = kind_bytes;
         }
         max_it = cs.max_it;
         tol = cs.tol;
@@ -298,12 +307,23 @@ struct dalm_handle {
             for (int a = 0; a < 3; a++) {
                 const std::vector<double> &x = *ctr[a], &d = *wid[a];
                 std::vector<float4> t(x.size(), make_float4(0.f, 0.f, 0.f, 0.f));
+                std::vector<float2> w(x.size());
+                std::vector<double2> r(x.size(), make_double2(0.0, 0.0));
+                for (size_t n = 0; n < x.size(); n++) {
+                    const double cb = std::cbrt(d[n]);
+                    w[n] = make_float2((float)d[n], (float)(cb * cb));
+                    if (n + 1 < x.size()) r[n].x = 1.0 / (x[n + 1] - x[n]);
+                    if (n >= 1 && n + 1 < x.size()) r[n].y = 1.0 / (x[n + 1] - x[n - 1]);
+                }
                 for (size_t n = 1; n + 1 < x.size(); n++)
                     t[n] = make_float4((float)(1.0 / d[n]), (float)(1.0 / (x[n + 1] - x[n])),
                                        (float)(1.0 / (x[n] - x[n - 1])),
                                        (float)(1.0 / (x[n + 1] - x[n - 1])));
                 geo.ax[a] = upload(t);
+                geo.wd[a] = upload(w);
+                geo.inv64[a] = upload(r);
             }
+            geo.cs2 = (float)(cs.cs * cs.cs);
         }
 
         size_t n = (size_t)g.total;
@@ -333,6 +353,18 @@ struct dalm_handle {
         // FP32 inner solves exist for BiCGStab only; SOR and Jacobi solves
         // stay FP64 under DALM_MIXED
         mixed = opt.precision == DALM_MIXED && pcfg.method == PM_BICG;
+        f32 = mixed && !opt.reference_sums;
+        if (f32) {
+            for (int b = 0; b < 2; b++)
+                for (int m = 0; m < 3; m++) {
+                    U32[b][m] = dalloc<float>(n);
+                    JU32[b][m] = dalloc<float>(n);
+                }
+            for (int m = 0; m < 3; m++) {
+                F32[m] = dalloc<float>(n);
+                DALM_CUDA(cudaMemset(F32[m], 0, sizeof(float) * n));
+            }
+        }
         if (mixed) {
             float **kv32[] = {&pbf.x, &pbf.r, &pbf.r0, &pbf.pk, &pbf.q, &pbf.s, &pbf.t,
                               &pbf.pp, &pbf.ss, &pbf.tp, &pbf.ts};
@@ -401,6 +433,7 @@ struct dalm_handle {
                                      cudaMemcpyHostToDevice));
             }
         }
+        narrow_state(false);
         refresh_after_state(DALM_SET_APPLY_UBC | DALM_SET_RECOMPUTE_JU, nullptr);
         DALM_CUDA(cudaStreamSynchronize(stream));
         if (opt.write_output) init_output();
@@ -610,20 +643,61 @@ struct dalm_handle {
     Vec3<double> ju_other() { return {{JU[1 - jcur][0], JU[1 - jcur][1], JU[1 - jcur][2]}}; }
     static Vec3<const double> c(Vec3<double> v) { return {{v.c[0], v.c[1], v.c[2]}}; }
     Vec3<double> f3() { return {{F[0], F[1], F[2]}}; }
+    Vec3<float> u32_cur() { return {{U32[ucur][0], U32[ucur][1], U32[ucur][2]}}; }
+    Vec3<float> u32_old() { return {{U32[1 - ucur][0], U32[1 - ucur][1], U32[1 - ucur][2]}}; }
+    Vec3<float> ju32_cur() { return {{JU32[jcur][0], JU32[jcur][1], JU32[jcur][2]}}; }
+    Vec3<float> ju32_other() { return {{JU32[1 - jcur][0], JU32[1 - jcur][1], JU32[1 - jcur][2]}}; }
+    Vec3<float> f32v() { return {{F32[0], F32[1], F32[2]}}; }
+    static Vec3<const float> c(Vec3<float> v) { return {{v.c[0], v.c[1], v.c[2]}}; }
+
+    // FP64 views of the FP32 stencil fields (DALM_MIXED): widen before the
+    // ABI or an FP64 kernel reads U, Uold, JU or f; narrow after the ABI
+    // wrote them (with_ju: JU too, else it is recomputed from U)
+    void widen_state() {
+        if (!f32 || !f64_stale) return;
+        const long long n = g.total;
+        for (int b = 0; b < 2; b++)
+            for (int m = 0; m < 3; m++) launch_widen(L, U32[b][m], U[b][m], n);
+        for (int m = 0; m < 3; m++) {
+            launch_widen(L, JU32[jcur][m], JU[jcur][m], n);
+            launch_widen(L, F32[m], F[m], n);
+        }
+        f64_stale = false;
+    }
+    void narrow_state(bool with_ju) {
+        if (!f32) return;
+        const long long n = g.total;
+        for (int b = 0; b < 2; b++)
+            for (int m = 0; m < 3; m++) launch_narrow(L, U[b][m], U32[b][m], n);
+        for (int m = 0; m < 3; m++) {
+            if (with_ju) {
+                launch_narrow(L, JU[jcur][m], JU32[jcur][m], n);
+                launch_narrow(L, JU[jcur][m], JU32[1 - jcur][m], n);
+            }
+            launch_narrow(L, F[m], F32[m], n);
+        }
+    }
 
     // ---- stages ----------------------------------------------------------
     void stage_predict() {
         StageTimer t(this, DALM_STAGE_PREDICT);
         P.fbox = fbox;
-        if (mixed)
-            launch_predict_f32(L, P, geo, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
-        else
+        if (f32) {
+            launch_predict32(L, P, geo, c(u32_cur()), u32_old(), c(ju32_cur()), c(f32v()));
+            f64_stale = true;
+        } else {
             launch_predict(L, P, c(u_cur()), u_old(), c(ju_cur()), c(f3()));
+        }
         ucur = 1 - ucur;  // the old buffer is now Uold
     }
     void stage_flux_rhs() {
         StageTimer t(this, DALM_STAGE_FLUX_RHS);
-        launch_flux_rhs(L, P, c(u_cur()), ju_cur(), B);
+        if (f32) {
+            launch_flux32(L, P, geo, c(u32_cur()), ju32_cur(), B);
+            f64_stale = true;
+        } else {
+            launch_flux_rhs(L, P, c(u_cur()), ju_cur(), B);
+        }
     }
     // iteration n (from 0) of the current solve
     void enqueue_poisson_iteration(long long n) {
@@ -817,9 +891,18 @@ struct dalm_handle {
     void stage_project() {
         StageTimer t(this, DALM_STAGE_PROJECT);
         launch_pressure_bc(L, P, Pp);
-        launch_project(L, P, u_cur(), ju_cur(), ju_other(), Pp, Partials<2>{partial, ticket}, d_diag);
-        jcur = 1 - jcur;
-        launch_velocity_bc(L, P, u_cur(), c(u_old()));
+        if (f32) {
+            launch_project32(L, P, geo, u32_cur(), c(ju32_cur()), ju32_other(), Pp,
+                             Partials<2>{partial, ticket}, d_diag);
+            jcur = 1 - jcur;
+            launch_velocity_bc(L, P, u32_cur(), c(u32_old()));
+            f64_stale = true;
+        } else {
+            launch_project(L, P, u_cur(), ju_cur(), ju_other(), Pp, Partials<2>{partial, ticket},
+                           d_diag);
+            jcur = 1 - jcur;
+            launch_velocity_bc(L, P, u_cur(), c(u_old()));
+        }
         DALM_CUDA(cudaMemcpyAsync(h_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToHost, stream));
     }
 
@@ -1003,6 +1086,12 @@ struct dalm_handle {
         if (opt.reference_sums) {
             alm_points_host(tm, c(u_cur()));
             alm_project_host();
+        } else if (f32) {
+            launch_alm_points(L, P, alm, tm, c(u32_cur()));
+            Box cur = force_box(tm);
+            launch_alm_project(L, P, alm, unite(fbox, cur), f32v());
+            fbox = cur;
+            f64_stale = true;
         } else {
             launch_alm_points(L, P, alm, tm, c(u_cur()));
             Box cur = force_box(tm);
@@ -1016,7 +1105,10 @@ struct dalm_handle {
     }
     void stage_diag() {
         StageTimer t(this, DALM_STAGE_DIAG);
-        launch_diag(L, P, c(u_cur()), c(ju_cur()), Partials<2>{partial, ticket}, d_diag);
+        if (f32)
+            launch_diag(L, P, c(u32_cur()), c(ju32_cur()), Partials<2>{partial, ticket}, d_diag);
+        else
+            launch_diag(L, P, c(u_cur()), c(ju_cur()), Partials<2>{partial, ticket}, d_diag);
         DALM_CUDA(cudaMemcpyAsync(h_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToHost, stream));
     }
     void stage_tavg() {
@@ -1026,7 +1118,10 @@ struct dalm_handle {
         StageTimer t(this, DALM_STAGE_TAVG);
         tavg_count++;
         double w = 1. / tavg_count;
-        launch_tavg(L, g, {{Utavg[0], Utavg[1], Utavg[2]}}, c(u_cur()), w);
+        if (f32)
+            launch_tavg(L, g, {{Utavg[0], Utavg[1], Utavg[2]}}, c(u32_cur()), w);
+        else
+            launch_tavg(L, g, {{Utavg[0], Utavg[1], Utavg[2]}}, c(u_cur()), w);
     }
 
     void run_stage(int s) {
@@ -1137,7 +1232,10 @@ struct dalm_handle {
         if (probe_list.empty() || !(t >= cs.output_start_time)) return;
         const int n = (int)probe_list.size();
         std::vector<double> v(3 * (size_t)n);
-        launch_gather_points(L, c(u_cur()), d_probe_idx, n, d_probe_val);
+        if (f32)
+            launch_gather_points(L, c(u32_cur()), d_probe_idx, n, d_probe_val);
+        else
+            launch_gather_points(L, c(u_cur()), d_probe_idx, n, d_probe_val);
         DALM_CUDA(cudaMemcpyAsync(v.data(), d_probe_val, sizeof(double) * v.size(),
                                   cudaMemcpyDeviceToHost, stream));
         DALM_CUDA(cudaStreamSynchronize(stream));
@@ -1174,6 +1272,7 @@ struct dalm_handle {
         }
         if (!(t - 0.5 * cs.dt < next_output_time && next_output_time <= t + 0.5 * cs.dt)) return;
         next_output_time += cs.output_interval_time;
+        widen_state();
         const size_t cells = (size_t)g.nx * g.ny * g.nz;
         std::vector<double> u(3 * cells), p(cells), dv(cells), q(cells), f(3 * cells);
         get_field(DALM_FIELD_U, u.data());
@@ -1199,6 +1298,30 @@ struct dalm_handle {
 
     // derived quantities after a state change (src/solver.h:767-833)
     void refresh_after_state(int flags, const double *JU_host) {
+        if (f32) {
+            // U (and p) were written to the FP64 views: narrow U, then derive
+            // on the FP32 fields
+            for (int m = 0; m < 3; m++) launch_narrow(L, U[ucur][m], U32[ucur][m], g.total);
+            if (flags & DALM_SET_APPLY_UBC) {
+                for (int m = 0; m < 3; m++)
+                    DALM_CUDA(cudaMemcpyAsync(U32[1 - ucur][m], U32[ucur][m], sizeof(float) * g.total,
+                                              cudaMemcpyDeviceToDevice, stream));
+                launch_velocity_bc(L, P, u32_cur(), c(u32_old()));
+            }
+            if ((flags & DALM_SET_RECOMPUTE_JU) || !JU_host) {
+                launch_flux32(L, P, geo, c(u32_cur()), ju32_cur(), nullptr);
+            } else {
+                upload_field(JU_host, 3, JU[jcur]);
+                for (int m = 0; m < 3; m++) {
+                    launch_narrow(L, JU[jcur][m], JU32[jcur][m], g.total);
+                    launch_narrow(L, JU[jcur][m], JU32[1 - jcur][m], g.total);
+                }
+            }
+            f64_stale = true;
+            stage_alm();
+            stage_diag();
+            return;
+        }
         if (flags & DALM_SET_APPLY_UBC) {
             for (int m = 0; m < 3; m++)
                 DALM_CUDA(cudaMemcpyAsync(U[1 - ucur][m], U[ucur][m], sizeof(double) * g.total,
@@ -1241,6 +1364,7 @@ struct dalm_handle {
     }
 
     void get_field(int which, double *out) {
+        widen_state();
         switch (which) {
         case DALM_FIELD_U: download_field(U[ucur], 3, out); break;
         case DALM_FIELD_UOLD: download_field(U[1 - ucur], 3, out); break;
@@ -1265,13 +1389,27 @@ struct dalm_handle {
         }
     }
     void set_field(int which, const double *in) {
+        // with FP32 stencil fields the FP64 copy is written, then rounded
+        // into the FP32 field the stages use
+        auto narrow3 = [&](double *const *src, float *const *dst) {
+            if (!f32) return;
+            for (int m = 0; m < 3; m++) launch_narrow(L, src[m], dst[m], g.total);
+            f64_stale = true;
+        };
+        widen_state();
         switch (which) {
-        case DALM_FIELD_U: upload_field(in, 3, U[ucur]); break;
-        case DALM_FIELD_UOLD: upload_field(in, 3, U[1 - ucur]); break;
-        case DALM_FIELD_JU: upload_field(in, 3, JU[jcur]); upload_field(in, 3, JU[1 - jcur]); break;
+        case DALM_FIELD_U: upload_field(in, 3, U[ucur]); narrow3(U[ucur], U32[ucur]); break;
+        case DALM_FIELD_UOLD: upload_field(in, 3, U[1 - ucur]); narrow3(U[1 - ucur], U32[1 - ucur]); break;
+        case DALM_FIELD_JU:
+            upload_field(in, 3, JU[jcur]);
+            upload_field(in, 3, JU[1 - jcur]);
+            narrow3(JU[jcur], JU32[jcur]);
+            narrow3(JU[jcur], JU32[1 - jcur]);
+            break;
         case DALM_FIELD_P: upload_field(in, 1, &Pp); break;
         case DALM_FIELD_F:
             upload_field(in, 3, F);
+            narrow3(F, F32);
             fbox = Box{{(int)cs.gc, (int)cs.gc, (int)cs.gc},
                        {g.nx - (int)cs.gc, g.ny - (int)cs.gc, g.nz - (int)cs.gc}};
             break;
@@ -1279,6 +1417,7 @@ struct dalm_handle {
         case DALM_FIELD_UTAVG: upload_field(in, 3, Utavg); break;
         default: throw std::invalid_argument("field is derived and cannot be set");
         }
+        if (f32) DALM_CUDA(cudaStreamSynchronize(stream));
     }
 
     // ---- discrete adjoint of the time stepping ------------------------------
@@ -1474,6 +1613,9 @@ struct dalm_handle {
     }
 
     void power_gradient(int64_t t0, int64_t t1, int64_t k, double *grad_out, double *J_out) {
+        if (f32)
+            throw Unsupported("the discrete adjoint differentiates the FP64 form "
+                              "(DALM_FP64, or DALM_MIXED with reference_sums)");
         const int T = alm.wt_count;
         if (T == 0) throw Unsupported("the case has no turbines");
         if (k < 1) throw std::invalid_argument("ckpt_every must be at least 1");
@@ -1921,7 +2063,11 @@ int dalm_get_timings(dalm_handle *h, double ms[7], int64_t *launches, int reset)
     if (launches) *launches = h->launch_count;
     if (reset) {
         for (int s = 0; s < 7; s++) h->stage_ms[s] = 0;
-        for (int k = 0; k < KK_COUNT; k++) { h->kind_ms[k] = 0; h->kind_launches[k] = 0; }
+        for (int k = 0; k < KK_COUNT; k++) {
+            h->kind_ms[k] = 0;
+            h->kind_launches[k] = 0;
+            h->kind_bytes[k] = 0;
+        }
         h->launch_count = 0;
     }
     API_END(h)
@@ -1946,13 +2092,15 @@ int dalm_get_kernel_timing(dalm_handle *h, int index, const char **name, int64_t
                         : (double)(h->fbox.hi[0] - h->fbox.lo[0]) * (h->fbox.hi[1] - h->fbox.lo[1]) *
                               (h->fbox.hi[2] - h->fbox.lo[2]);
         double s = 0;
+        // the stencil fields U, JU, f: 8 bytes, or 4 as the mixed form's FP32 fields
+        const double v = h->f32 ? 0.5 : 1.0;
         switch (index) {
-        case KK_PREDICT: s = 9 * n + 3 * fcells + 6 * (stored - n); break;
-        case KK_FLUX_RHS: s = 7 * n; break;
-        case KK_PROJECT: s = 13 * n; break;
-        case KK_DIAG: s = 6 * n; break;
-        case KK_TAVG: s = 9 * stored; break;
-        case KK_ALM_PROJECT: s = 3 * fcells; break;
+        case KK_PREDICT: s = h->f32 ? v * (9 * n + 3 * fcells) : 9 * n + 3 * fcells + 6 * (stored - n); break;
+        case KK_FLUX_RHS: s = 6 * v * n + n; break;       // R U; W JU (stencil fields), b (FP64)
+        case KK_PROJECT: s = 12 * v * n + n; break;       // R U, JU, p; W U, JU
+        case KK_DIAG: s = 6 * v * n; break;
+        case KK_TAVG: s = (6 + 3 * v) * stored; break;    // R Utavg, U; W Utavg
+        case KK_ALM_PROJECT: s = 3 * v * fcells; break;
         case KK_SOR_SWEEP: s = 2 * n; break;
         case KK_RESIDUAL_NORM: s = (h->pcfg.method == PM_JACOBI ? 3 : 2) * n; break;
         case KK_JACOBI_SWEEP: s = 3 * n; break;
@@ -1977,6 +2125,10 @@ int dalm_get_kernel_timing(dalm_handle *h, int index, const char **name, int64_t
         default: s = 0; break;
         }
         *bytes_per_launch = 8.0 * s;
+        // kinds whose launches differ in size (the multigrid levels) count
+        // their bytes at launch time
+        if (h->kind_bytes[index] > 0 && h->kind_launches[index] > 0)
+            *bytes_per_launch = h->kind_bytes[index] / (double)h->kind_launches[index];
     }
     API_END(h)
 }

@@ -92,15 +92,27 @@ __device__ inline void warp_serial_sums(const Grid &g, Term term, double (&total
 // ---- flow kernels (flow_fp64.cu) ----
 void launch_predict(const LaunchCtx &L, const StepParams &P, Vec3<const double> uold,
                     Vec3<double> unew, Vec3<const double> ju, Vec3<const double> f);
-// the mixed-precision form's predictor: the increment in FP32 (flow_mixed.cu)
-// with the mesh as one FP32 table per axis: for stored index n,
-// {1/d_n, 1/(x_{n+1} - x_n), 1/(x_n - x_{n-1}), 1/(x_{n+1} - x_{n-1})}
+// The mixed-precision form's flow stages on FP32 stencil fields
+// (flow_mixed.cu).  Mesh tables per axis, for stored index n:
+//   ax    FP32 {1/d_n, 1/(x_{n+1} - x_n), 1/(x_n - x_{n-1}), 1/(x_{n+1} - x_{n-1})}
+//   wd    FP32 {d_n, cbrt(d_n)^2}  (face areas; the Smagorinsky filter width
+//         (Cs cbrt(dx dy dz))^2 = cs2 * wd_x.y * wd_y.y * wd_z.y)
+//   inv64 FP64 {1/(x_{n+1} - x_n), 1/(x_{n+1} - x_{n-1})}  (the projection)
 struct MixedGeom {
     const float4 *ax[3];
+    const float2 *wd[3];
+    const double2 *inv64[3];
+    float cs2;
 };
-void launch_predict_f32(const LaunchCtx &L, const StepParams &P, const MixedGeom &geo,
-                        Vec3<const double> uold, Vec3<double> unew, Vec3<const double> ju,
-                        Vec3<const double> f);
+void launch_predict32(const LaunchCtx &L, const StepParams &P, const MixedGeom &geo,
+                      Vec3<const float> uold, Vec3<float> unew, Vec3<const float> ju,
+                      Vec3<const float> f);
+// face fluxes and, with b non-null, the FP64 Poisson right-hand side
+void launch_flux32(const LaunchCtx &L, const StepParams &P, const MixedGeom &geo,
+                   Vec3<const float> u, Vec3<float> ju, double *b);
+void launch_project32(const LaunchCtx &L, const StepParams &P, const MixedGeom &geo, Vec3<float> u,
+                      Vec3<const float> ju_in, Vec3<float> ju_out, const double *p,
+                      Partials<2> part, DiagState *diag);
 void launch_flux_rhs(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                      Vec3<double> ju, double *b);
 void launch_flux_only(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
@@ -109,16 +121,20 @@ void launch_pressure_bc(const LaunchCtx &L, const StepParams &P, double *p);
 void launch_project(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
                     Vec3<double> ju_in, Vec3<double> ju_out, const double *p, Partials<2> part,
                     DiagState *diag);
-void launch_velocity_bc(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
-                        Vec3<const double> uold);
+// apply_Ubc on FP64 (T = double) or FP32 (T = float, the mixed form's
+// stencil fields) storage; FP64 arithmetic either way
+template <typename T>
+void launch_velocity_bc(const LaunchCtx &L, const StepParams &P, Vec3<T> u, Vec3<const T> uold);
 void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                  Vec3<const double> ju, Partials<2> part, DiagState *diag);
+void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const float> u,
+                 Vec3<const float> ju, Partials<2> part, DiagState *diag);
 void launch_nut_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> u, double *nut);
 void launch_div_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> ju, double *div);
 // Q-criterion of U on the interior (calc_q, src/cfd.h:949-1034)
 void launch_q_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> u, double *q);
-void launch_tavg(const LaunchCtx &L, const Grid &g, Vec3<double> tavg, Vec3<const double> u,
-                 double w);
+template <typename T>
+void launch_tavg(const LaunchCtx &L, const Grid &g, Vec3<double> tavg, Vec3<const T> u, double w);
 // reference AoS/scalar layout <-> device SoA layout (ncomp = 1 or 3)
 void launch_to_device_layout(const LaunchCtx &L, const Grid &g, const double *ref, int ncomp,
                              double *const *dst);
@@ -126,7 +142,11 @@ void launch_to_ref_layout(const LaunchCtx &L, const Grid &g, double *const *src,
                           double *ref);
 void launch_fill(const LaunchCtx &L, double *p, long long n, double v);
 // out[3 t + m] = U_m at device index idx[t] (probe sampling)
-void launch_gather_points(const LaunchCtx &L, Vec3<const double> u, const long long *idx, int n,
+template <typename T>
+void launch_gather_points(const LaunchCtx &L, Vec3<const T> u, const long long *idx, int n,
                           double *out);
+// dst[x] = src[x] over n elements (FP32 <-> FP64 copies of a field)
+void launch_widen(const LaunchCtx &L, const float *src, double *dst, long long n);
+void launch_narrow(const LaunchCtx &L, const double *src, float *dst, long long n);
 
 }  // namespace dalm

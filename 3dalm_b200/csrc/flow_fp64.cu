@@ -346,27 +346,30 @@ k_project(StepParams P, Segments T, Vec3<double> U, Vec3<double> JUin, Vec3<doub
 
 // divergence of cell c from the face fluxes (src/cfd.h:1093-1105) and the
 // cell CFL number (src/cfd.h:1126-1130)
-__device__ __forceinline__ double cell_div(const StepParams &P, Vec3<const double> JU, int i,
-                                           int j, int k) {
+template <typename T>
+__device__ __forceinline__ double cell_div(const StepParams &P, Vec3<const T> JU, int i, int j,
+                                           int k) {
     const Grid &g = P.g;
     long long c = g.at(i, j, k);
     double J = P.m.dx[i] * P.m.dy[j] * P.m.dz[k];
-    return (JU.c[0][c] - JU.c[0][g.at(i - 1, j, k)] + JU.c[1][c] - JU.c[1][g.at(i, j - 1, k)] +
-            JU.c[2][c] - JU.c[2][c - 1]) / J;
+    return ((double)JU.c[0][c] - (double)JU.c[0][g.at(i - 1, j, k)] + (double)JU.c[1][c] -
+            (double)JU.c[1][g.at(i, j - 1, k)] + (double)JU.c[2][c] - (double)JU.c[2][c - 1]) / J;
 }
-__device__ __forceinline__ double cell_cfl(const StepParams &P, Vec3<const double> U, int i,
-                                           int j, int k) {
+template <typename T>
+__device__ __forceinline__ double cell_cfl(const StepParams &P, Vec3<const T> U, int i, int j,
+                                           int k) {
     long long c = P.g.at(i, j, k);
-    return fabs(U.c[0][c]) * P.dt / P.m.dx[i] + fabs(U.c[1][c]) * P.dt / P.m.dy[j] +
-           fabs(U.c[2][c]) * P.dt / P.m.dz[k];
+    return fabs((double)U.c[0][c]) * P.dt / P.m.dx[i] + fabs((double)U.c[1][c]) * P.dt / P.m.dy[j] +
+           fabs((double)U.c[2][c]) * P.dt / P.m.dz[k];
 }
 
 // Diagnostics alone (after set_state): sum div^2 and max CFL.
+template <typename T>
 __global__ void __launch_bounds__(TILE_THREADS)
-k_diag(StepParams P, Segments T, Vec3<const double> U, Vec3<const double> JU, Partials<2> part,
+k_diag(StepParams P, Segments S, Vec3<const T> U, Vec3<const T> JU, Partials<2> part,
        DiagState *diag) {
     double div2 = 0, cfl = 0;
-    TILE_LOOP(T)
+    TILE_LOOP(S)
         double d = cell_div(P, JU, i, j, k);
         div2 += d * d;
         double local = cell_cfl(P, U, i, j, k);
@@ -429,7 +432,10 @@ __device__ __forceinline__ double quad_poly(double x0, double x1, double x2, dou
 // outflow on Uold, slip y-/y+/z+, no-slip z-.  One thread per face column;
 // each writes the gc guide cells of its column.  Reads only interior cells
 // of U and the old guide values, so the faces are independent.
-__global__ void k_velocity_bc(StepParams P, Vec3<double> U, Vec3<const double> V) {
+// T is the storage type of U (double; float for the FP32 stencil fields of
+// the mixed form): the arithmetic is FP64 either way.
+template <typename T>
+__global__ void k_velocity_bc(StepParams P, Vec3<T> U, Vec3<const T> V) {
     const Grid &g = P.g;
     int GC = g.gc;
     long long nyz = (long long)g.nj() * g.nk(), nxz = (long long)g.ni() * g.nk(),
@@ -446,19 +452,19 @@ __global__ void k_velocity_bc(StepParams P, Vec3<double> U, Vec3<const double> V
                 for (int i = 0; i < GC; i++) {
                     long long id = g.at(i, j, k);
                     for (int m = 0; m < 3; m++)
-                        U.c[m][id] = P.prof ? P.prof[((long long)j * g.nz + k) * 3 + m] : P.uin[m];
+                        U.c[m][id] = (T)(P.prof ? P.prof[((long long)j * g.nz + k) * 3 + m] : P.uin[m]);
                 }
             } else {
                 for (int i = g.nx - GC; i < g.nx; i++) {
                     long long i0 = g.at(i, j, k), i1 = g.at(i - 1, j, k), i2 = g.at(i - 2, j, k);
-                    double uout = U.c[0][i0];
+                    double uout = (double)U.c[0][i0];
                     double nv[3];
                     for (int m = 0; m < 3; m++) {
-                        double f0 = V.c[m][i0], f1 = V.c[m][i1], f2 = V.c[m][i2];
+                        double f0 = (double)V.c[m][i0], f1 = (double)V.c[m][i1], f2 = (double)V.c[m][i2];
                         double grad = (3 * f0 - 4 * f1 + f2) / 2;
                         nv[m] = f0 - uout * P.dt * grad / P.m.dx[i];
                     }
-                    for (int m = 0; m < 3; m++) U.c[m][i0] = nv[m];
+                    for (int m = 0; m < 3; m++) U.c[m][i0] = (T)nv[m];
                 }
             }
             continue;
@@ -475,11 +481,11 @@ __global__ void k_velocity_bc(StepParams P, Vec3<double> U, Vec3<const double> V
             double y0 = P.m.y[j0], y1 = P.m.y[j1];
             double y2 = side ? P.m.y[j1] + 0.5 * P.m.dy[j1] : P.m.y[j1] - 0.5 * P.m.dy[j1];
             double y3 = P.m.y[j3], y4 = P.m.y[j4];
-            double ubc[3] = {U.c[0][a1], 0, U.c[2][a1]};
+            double ubc[3] = {(double)U.c[0][a1], 0, (double)U.c[2][a1]};
             for (int m = 0; m < 3; m++) {
-                double f0 = U.c[m][a0], f1 = U.c[m][a1], f2 = ubc[m];
-                U.c[m][a3] = quad_poly(y0, y1, y2, f0, f1, f2, y3);
-                U.c[m][a4] = quad_poly(y0, y1, y2, f0, f1, f2, y4);
+                double f0 = (double)U.c[m][a0], f1 = (double)U.c[m][a1], f2 = ubc[m];
+                U.c[m][a3] = (T)quad_poly(y0, y1, y2, f0, f1, f2, y3);
+                U.c[m][a4] = (T)quad_poly(y0, y1, y2, f0, f1, f2, y4);
             }
             continue;
         }
@@ -498,13 +504,13 @@ __global__ void k_velocity_bc(StepParams P, Vec3<double> U, Vec3<const double> V
         // z+ slip; z- no slip, or slip upstream of a retracted floor's start
         // (src/bc.h:140-160)
         if (side || (P.retracted && P.m.x[i] < P.floor_start)) {
-            ubc[0] = U.c[0][a1];
-            ubc[1] = U.c[1][a1];
+            ubc[0] = (double)U.c[0][a1];
+            ubc[1] = (double)U.c[1][a1];
         }
         for (int m = 0; m < 3; m++) {
-            double f0 = U.c[m][a0], f1 = U.c[m][a1], f2 = ubc[m];
-            U.c[m][a3] = quad_poly(z0, z1, z2, f0, f1, f2, z3);
-            U.c[m][a4] = quad_poly(z0, z1, z2, f0, f1, f2, z4);
+            double f0 = (double)U.c[m][a0], f1 = (double)U.c[m][a1], f2 = ubc[m];
+            U.c[m][a3] = (T)quad_poly(z0, z1, z2, f0, f1, f2, z3);
+            U.c[m][a4] = (T)quad_poly(z0, z1, z2, f0, f1, f2, z4);
         }
     }
 }
@@ -556,7 +562,8 @@ k_q_field(StepParams P, Segments T, Vec3<const double> U, double *q) {
 
 // Running time average over every stored cell (calc_ax_plus_by,
 // src/mv.h:322-335 as used at src/solver.h:1198-1203).
-__global__ void k_tavg(Grid g, Vec3<double> A, Vec3<const double> U, double w) {
+template <typename T>
+__global__ void k_tavg(Grid g, Vec3<double> A, Vec3<const T> U, double w) {
     long long tot = (long long)g.nx * g.ny * g.nz;
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < tot;
          n += (long long)gridDim.x * blockDim.x) {
@@ -564,7 +571,7 @@ __global__ void k_tavg(Grid g, Vec3<double> A, Vec3<const double> U, double w) {
         long long r = n / g.nz;
         int j = (int)(r % g.ny), i = (int)(r / g.ny);
         long long c = g.at(i, j, k);
-        for (int m = 0; m < 3; m++) A.c[m][c] = (1. - w) * A.c[m][c] + w * U.c[m][c];
+        for (int m = 0; m < 3; m++) A.c[m][c] = (1. - w) * A.c[m][c] + w * (double)U.c[m][c];
     }
 }
 
@@ -626,10 +633,23 @@ int plane_blocks(const Grid &g) {
     return (int)(b < 4096 ? (b > 0 ? b : 1) : 4096);
 }
 
-__global__ void k_gather_points(Vec3<const double> U, const long long *idx, int n, double *out) {
+template <typename T>
+__global__ void k_gather_points(Vec3<const T> U, const long long *idx, int n, double *out) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    for (int m = 0; m < 3; m++) out[3 * t + m] = U.c[m][idx[t]];
+    for (int m = 0; m < 3; m++) out[3 * t + m] = (double)U.c[m][idx[t]];
+}
+
+// element-wise precision conversions over whole allocations (same layout)
+__global__ void k_widen(const float *src, double *dst, long long n) {
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n;
+         x += (long long)gridDim.x * blockDim.x)
+        dst[x] = (double)src[x];
+}
+__global__ void k_narrow(const double *src, float *dst, long long n) {
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n;
+         x += (long long)gridDim.x * blockDim.x)
+        dst[x] = (float)src[x];
 }
 
 }  // namespace
@@ -679,12 +699,16 @@ void launch_project(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
     }
 }
 
-void launch_velocity_bc(const LaunchCtx &L, const StepParams &P, Vec3<double> u,
-                        Vec3<const double> uold) {
+template <typename T>
+void launch_velocity_bc(const LaunchCtx &L, const StepParams &P, Vec3<T> u, Vec3<const T> uold) {
     L.pre(KK_UBC);
-    k_velocity_bc<<<plane_blocks(P.g), 256, 0, L.s>>>(P, u, uold);
+    k_velocity_bc<T><<<plane_blocks(P.g), 256, 0, L.s>>>(P, u, uold);
     L.post(KK_UBC);
 }
+template void launch_velocity_bc<double>(const LaunchCtx &, const StepParams &, Vec3<double>,
+                                         Vec3<const double>);
+template void launch_velocity_bc<float>(const LaunchCtx &, const StepParams &, Vec3<float>,
+                                        Vec3<const float>);
 
 void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
                  Vec3<const double> ju, Partials<2> part, DiagState *diag) {
@@ -693,7 +717,15 @@ void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const double> u,
     if (P.reference_sums)
         k_seq_diag<<<1, 32, 0, L.s>>>(P, u, ju, diag);
     else
-        k_diag<<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju, part, diag);
+        k_diag<double><<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju, part, diag);
+    L.post(KK_DIAG);
+}
+
+void launch_diag(const LaunchCtx &L, const StepParams &P, Vec3<const float> u,
+                 Vec3<const float> ju, Partials<2> part, DiagState *diag) {
+    Segments T = Segments::make(interior_box(P.g), L.blocks);
+    L.pre(KK_DIAG);
+    k_diag<float><<<L.blocks, TILE_THREADS, 0, L.s>>>(P, T, u, ju, part, diag);
     L.post(KK_DIAG);
 }
 
@@ -718,12 +750,16 @@ void launch_q_field(const LaunchCtx &L, const StepParams &P, Vec3<const double> 
     L.post(KK_LAYOUT);
 }
 
-void launch_tavg(const LaunchCtx &L, const Grid &g, Vec3<double> tavg, Vec3<const double> u,
-                 double w) {
+template <typename T>
+void launch_tavg(const LaunchCtx &L, const Grid &g, Vec3<double> tavg, Vec3<const T> u, double w) {
     L.pre(KK_TAVG);
-    k_tavg<<<L.blocks, 256, 0, L.s>>>(g, tavg, u, w);
+    k_tavg<T><<<L.blocks, 256, 0, L.s>>>(g, tavg, u, w);
     L.post(KK_TAVG);
 }
+template void launch_tavg<double>(const LaunchCtx &, const Grid &, Vec3<double>,
+                                  Vec3<const double>, double);
+template void launch_tavg<float>(const LaunchCtx &, const Grid &, Vec3<double>, Vec3<const float>,
+                                 double);
 
 void launch_to_device_layout(const LaunchCtx &L, const Grid &g, const double *ref, int ncomp,
                              double *const *dst) {
@@ -741,11 +777,27 @@ void launch_to_ref_layout(const LaunchCtx &L, const Grid &g, double *const *src,
     L.post(KK_LAYOUT);
 }
 
-void launch_gather_points(const LaunchCtx &L, Vec3<const double> u, const long long *idx, int n,
+template <typename T>
+void launch_gather_points(const LaunchCtx &L, Vec3<const T> u, const long long *idx, int n,
                           double *out) {
     if (n <= 0) return;
     L.pre(KK_LAYOUT);
-    k_gather_points<<<(n + 127) / 128, 128, 0, L.s>>>(u, idx, n, out);
+    k_gather_points<T><<<(n + 127) / 128, 128, 0, L.s>>>(u, idx, n, out);
+    L.post(KK_LAYOUT);
+}
+template void launch_gather_points<double>(const LaunchCtx &, Vec3<const double>,
+                                           const long long *, int, double *);
+template void launch_gather_points<float>(const LaunchCtx &, Vec3<const float>, const long long *,
+                                          int, double *);
+
+void launch_widen(const LaunchCtx &L, const float *src, double *dst, long long n) {
+    L.pre(KK_LAYOUT);
+    k_widen<<<L.blocks, 256, 0, L.s>>>(src, dst, n);
+    L.post(KK_LAYOUT);
+}
+void launch_narrow(const LaunchCtx &L, const double *src, float *dst, long long n) {
+    L.pre(KK_LAYOUT);
+    k_narrow<<<L.blocks, 256, 0, L.s>>>(src, dst, n);
     L.post(KK_LAYOUT);
 }
 

@@ -661,6 +661,8 @@ struct DeviceCycle {
         L.pre(KK_MG_SMOOTH);
         zline_dispatch(L, a, st);
         L.post(KK_MG_SMOOTH);
+        // R f and the other colour's x, W this colour's x: half the level each
+        L.bytes(KK_MG_SMOOTH, 4.0 * 1.5 * (double)M.L[l].cells());
         last_color[l] = color;
     }
     void restrict(int l) {
@@ -668,6 +670,9 @@ struct DeviceCycle {
         k_mg_restrict<<<blocks_for(M.L[l + 1].cells(), L.blocks), MG_THREADS, 0, L.s>>>(
             M.L[l], M.L[l + 1], M.x[l], M.f[l], M.f[l + 1], last_color[l], st);
         L.post(KK_MG_TRANSFER);
+        // R x, f of half the children; W the coarse f
+        L.bytes(KK_MG_TRANSFER, 4.0 * ((double)M.L[l].cells() + 0.5 * (double)M.L[l].cells() +
+                                       (double)M.L[l + 1].cells()));
     }
     void coarse() {
         const int l = M.levels - 1;
@@ -675,6 +680,7 @@ struct DeviceCycle {
         k_mg_coarse<<<blocks_for((long long)M.ncoarse * 32, L.blocks), MG_THREADS, 0, L.s>>>(
             M.L[l], M.kinv, M.ncoarse, M.f[l], M.x[l], st);
         L.post(KK_MG_COARSE);
+        L.bytes(KK_MG_COARSE, 4.0 * ((double)M.ncoarse * M.ncoarse + 2.0 * M.ncoarse));
     }
     void prolong(int l) { pending[l] = true; }
 };
@@ -697,9 +703,11 @@ void launch_mg_begin(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B, dou
                      Partials<1> part, KrylovState *st) {
     const MgLevel &v = M.L[0];
     const int nb = blocks_for(v.cells(), L.blocks);
+    const double n = (double)v.cells();
     L.pre(KK_MG_PCG);
     k_mg_rhs<<<nb, MG_THREADS, 0, L.s>>>(v, B.r, B.e, (float)max_diag, st);
     L.post(KK_MG_PCG);
+    L.bytes(KK_MG_PCG, 12.0 * n);  // R r; W r, e
     MgDev m = M;
     m.f[0] = B.r;
     m.x[0] = B.z;
@@ -707,17 +715,21 @@ void launch_mg_begin(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B, dou
     L.pre(KK_MG_PCG);
     k_mg_first<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.r, B.z, B.p, part, st);
     L.post(KK_MG_PCG);
+    L.bytes(KK_MG_PCG, 12.0 * n);  // R r, z; W p
 }
 
 void launch_mg_iteration(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B,
                          double max_diag, Partials<1> part, KrylovState *st) {
     const MgLevel &v = M.L[0];
+    const double n = (double)v.cells();
     L.pre(KK_MG_PCG);
     k_mg_spmv<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st);
     L.post(KK_MG_PCG);
+    L.bytes(KK_MG_PCG, 8.0 * n);  // R p; W q
     L.pre(KK_MG_PCG);
     k_mg_update<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.e, B.r, B.p, B.q, (float)max_diag, part, st);
     L.post(KK_MG_PCG);
+    L.bytes(KK_MG_PCG, 24.0 * n);  // R e, p, r, q; W e, r
     MgDev m = M;
     m.f[0] = B.r;
     m.x[0] = B.z;
@@ -725,9 +737,11 @@ void launch_mg_iteration(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B,
     L.pre(KK_MG_PCG);
     k_mg_rz<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.r, B.z, part, st);
     L.post(KK_MG_PCG);
+    L.bytes(KK_MG_PCG, 8.0 * n);  // R r, z
     L.pre(KK_MG_PCG);
     k_mg_pupdate<<<blocks_for(v.cells(), L.blocks), MG_THREADS, 0, L.s>>>(v, B.z, B.p, st);
     L.post(KK_MG_PCG);
+    L.bytes(KK_MG_PCG, 12.0 * n);  // R z, p; W p
 }
 
 }  // namespace dalm

@@ -94,13 +94,40 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision timing")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost run")
+    ap.add_argument("--compare-forms", type=int, default=0, metavar="STEPS",
+                    help="instead of the benchmark: run the FP64 and the mixed-precision form "
+                         "from the same initial state for STEPS steps and print their "
+                         "time-averaged turbine power, final field differences and wall times")
+    ap.add_argument("--avg-from", type=int, default=1,
+                    help="first step of the --compare-forms power average")
     return ap.parse_args()
 
 
-def mixed_errors(a, b):
+def grad_interior(p, mesh, gc):
+    """Central differences of a cell field over the interior cells along x,
+    y, z with the cell-centre coordinates (the pressure gradient the
+    projection applies, src/cfd.h:601-783)."""
+    import numpy as np
+    out = []
+    for a in range(3):
+        c = mesh[a]
+        n = p.shape[a]
+        sl = [slice(gc, p.shape[b] - gc) for b in range(3)]
+        hi, lo = list(sl), list(sl)
+        hi[a], lo[a] = slice(gc + 1, n - gc + 1), slice(gc - 1, n - gc - 1)
+        shape = [1, 1, 1]
+        shape[a] = n - 2 * gc
+        h = (c[gc + 1:n - gc + 1] - c[gc - 1:n - gc - 1]).reshape(shape)
+        out.append((p[tuple(hi)] - p[tuple(lo)]) / h)
+    return np.stack(out, axis=-1)
+
+
+def mixed_errors(a, b, mesh=None, gc=2):
     """Relative L2 error of the mixed form's final state against the FP64
-    form's after the same steps: per velocity component, pressure, and per
-    turbine thrust / power."""
+    form's after the same steps: per velocity component; the pressure as
+    stored, with its mean removed, and its gradient (what the solver
+    tolerance pins: two solves that both meet the RMS residual tolerance may
+    differ in p's smooth modes); per turbine thrust / power."""
     import numpy as np
 
     def rel(x, y):
@@ -108,6 +135,11 @@ def mixed_errors(a, b):
         return float(np.linalg.norm(x - y) / (ny if ny > 0 else 1.0))
     out = {f"U[{m}]": rel(a["U"][..., m], b["U"][..., m]) for m in range(3)}
     out["p"] = rel(a["p"], b["p"])
+    inner = (slice(gc, -gc),) * 3
+    pa, pb = a["p"][inner], b["p"][inner]
+    out["p_mean_removed"] = rel(pa - pa.mean(), pb - pb.mean())
+    if mesh is not None:
+        out["grad_p"] = rel(grad_interior(a["p"], mesh, gc), grad_interior(b["p"], mesh, gc))
     (tha, _, pwa), (thb, _, pwb) = a["turbines"], b["turbines"]
     out["thrust"] = [float(abs(x - y) / abs(y)) if y else 0.0 for x, y in zip(tha, thb)]
     out["power"] = [float(abs(x - y) / abs(y)) if y else 0.0 for x, y in zip(pwa, pwb)]
@@ -238,10 +270,10 @@ def host_cores():
 # uncapped; the line says how many ran).  On the 16-core GPU hosts a whole
 # step of the 512x256x128 case takes ~0.15-0.25 s per BiCGStab iteration, and
 # the warm-up steps from the seeded state take ~3000 iterations.
-REF_BUDGET_S = float(os.environ.get("DALM_REF_BUDGET_S", "900"))
+REF_BUDGET_S = float(os.environ.get("DALM_REF_BUDGET_S", "720"))
 
 
-def run_reference_ranks(case, warmup, steps, ranks, max_it=None, budget=0.0, timeout=3000):
+def run_reference_ranks(case, warmup, steps, ranks, max_it=None, budget=0.0, timeout=1700):
     """The reference's own time step (oracle/_ref/ref_mpirun: the reference
     compiled from its sources, OpenACC off, with a shared-memory MPI subset)
     as `ranks` MPI ranks on the host cores: the 3-turbine case from its seeded
@@ -396,9 +428,12 @@ def run_ours(args):
             torch.distributed.barrier()
 
     def fresh_solver(profile, precision=pkg.FP64, inner=pkg.INNER_MULTIGRID):
-        """A solver at the start of the timed steps: state set, warm-up run."""
+        """A solver at the start of the timed steps: state set, warm-up run.
+        A profiled solver polls the pressure solve after every iteration
+        (no iteration is enqueued past convergence), so its per-kernel
+        launch counts and bytes are exact."""
         sv = pkg.Solver(tmp, device=local, profile=profile, precision=precision,
-                        mixed_inner=inner)
+                        mixed_inner=inner, poisson_batch=1 if profile else 0)
         sv.set_inflow_profile(prof)
         sv.set_state(U0)
         sv.step(max(args.warmup, 1))
@@ -431,7 +466,8 @@ def run_ours(args):
         ms = e0.elapsed_time(e1)
         _, launches = s.timings()
         ms = max_over_ranks(ms, world)
-        final = {"U": s.field("U"), "p": s.field("p"), "turbines": s.turbines()}
+        final = {"U": s.field("U"), "p": s.field("p"), "turbines": s.turbines(),
+                 "mesh": s.mesh(), "gc": s.gc}
         s.finalize()
         return ms, its, errs, clk, launches, final
 
@@ -447,7 +483,7 @@ def run_ours(args):
                  "vs_fp64": mvalue / value, "poisson_iterations": mits,
                  "max_residual": max(merrs), "fp64_max_residual": max(errs),
                  "tolerance": spec.tol, "clocks": mclk,
-                 "error_vs_fp64": mixed_errors(finalm, final64),
+                 "error_vs_fp64": mixed_errors(finalm, final64, final64["mesh"], final64["gc"]),
                  "how": "DALM_MIXED: FP64 iterative refinement (FP64 residual, norm, pressure "
                         "update and stop test) with capped FP32 inner passes of conjugate "
                         "gradients preconditioned by a geometric multigrid V-cycle; FP64 "
@@ -460,7 +496,8 @@ def run_ours(args):
         mixed["bicgstab_inner"] = {"value": bvalue, "vs_fp64": bvalue / value,
                                    "ms_per_step": bms / args.steps, "poisson_iterations": bits,
                                    "max_residual": max(berrs),
-                                   "error_vs_fp64": mixed_errors(finalb, final64)}
+                                   "error_vs_fp64": mixed_errors(finalb, final64,
+                                                                 final64["mesh"], final64["gc"])}
 
     # ---- end to end through the public API with host (pinned) buffers: a
     # second solver replays the same warm-up and the same timed steps, each
@@ -497,25 +534,54 @@ def run_ours(args):
 
     # ---- per-kernel device times: a replay of the same steps with CUDA
     # events around every launch on the solver's stream
-    s = fresh_solver(True)
-    s.timings(reset=True)
-    prof_its = []
-    for _ in range(args.steps):
-        s.step(1)
-        prof_its.append(s.stats()["it"])
-    kt = s.kernel_timings()
-    stage_ms, _ = s.timings()
-    if prof_its != its:
-        raise RuntimeError(f"profiled replay took other iteration counts {prof_its} than {its}")
+    def profiled_replay(precision, expect_its):
+        sv = fresh_solver(True, precision)
+        sv.timings(reset=True)
+        p_its = []
+        for _ in range(args.steps):
+            sv.step(1)
+            p_its.append(sv.stats()["it"])
+        kt_ = sv.kernel_timings()
+        st_ms, _ = sv.timings()
+        if p_its != expect_its:
+            raise RuntimeError(f"profiled replay took other iteration counts {p_its} than "
+                               f"{expect_its}")
+        return sv, kt_, st_ms
 
-    # ---- roofline of the dominant kernel
-    dom = max((k for k in kt if kt[k]["launches"] > 0 and kt[k]["bytes_per_launch"] > 0),
-              key=lambda k: kt[k]["ms"])
-    d = kt[dom]
-    per_launch_s = d["ms"] / d["launches"] / 1e3
-    achieved = d["bytes_per_launch"] / per_launch_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profiled_traffic(dom)
+
+    def roofline(kt_, step_ms, traffic_of=None):
+        """The kernel with the largest device time (algorithmic bytes per
+        launch / mean launch time) and the whole step (all kernels' bytes
+        per step / the unprofiled step time), against the measured peak."""
+        dom_ = max((k for k in kt_ if kt_[k]["launches"] > 0 and kt_[k]["bytes_per_launch"] > 0),
+                   key=lambda k: kt_[k]["ms"])
+        d_ = kt_[dom_]
+        pl = d_["ms"] / d_["launches"] / 1e3
+        ach = d_["bytes_per_launch"] / pl / 1e9
+        step_bytes = sum(v["launches"] * v["bytes_per_launch"] for v in kt_.values()) / args.steps
+        step_ach = step_bytes / (step_ms / 1e3) / 1e9
+        return {"bound": "hbm", "kernel": dom_, "achieved": ach, "peak": peak,
+                "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s", "frac": ach / peak,
+                "traffic": traffic_of(dom_) if traffic_of else None,
+                "algorithmic_bytes_per_launch": d_["bytes_per_launch"], "launch_us": pl * 1e6,
+                "launches": d_["launches"],
+                "share_of_kernel_time": d_["ms"] / max(1e-9, sum(v["ms"] for v in kt_.values())),
+                "step": {"algorithmic_bytes": step_bytes, "ms": step_ms,
+                         "achieved": step_ach, "frac": step_ach / peak},
+                "kernels": {k: {"launches": v["launches"], "ms_per_step": v["ms"] / args.steps,
+                                "achieved_gbs": (v["launches"] * v["bytes_per_launch"] /
+                                                 (v["ms"] / 1e3) / 1e9) if v["ms"] > 0 else None}
+                            for k, v in kt_.items() if v["launches"] > 0}}
+
+    if mixed is not None:
+        sm, mkt, _ = profiled_replay(pkg.MIXED, mixed["poisson_iterations"])
+        sm.finalize()
+        mixed["roofline"] = roofline(mkt, mixed["ms_per_step"])
+
+    s, kt, stage_ms = profiled_replay(pkg.FP64, its)
+    rl = roofline(kt, ms / args.steps, profiled_traffic)
+    dom = rl["kernel"]
     n_launch = int(launches)  # launches in the unprofiled timed region
 
     line = {
@@ -528,12 +594,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": h2d, "steps": e2e_steps,
                 "how": "per step: dalm_set_field(U,p) from pinned host, dalm_step(1), "
                        "dalm_get_field(U,p) to pinned host, dalm_get_step_stats; wall clock"},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "peak_source": f"{peak_kind} hbm_gbs", "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": d["bytes_per_launch"],
-                     "launch_us": per_launch_s * 1e6, "launches": d["launches"],
-                     "share_of_kernel_time": d["ms"] / max(1e-9, sum(v["ms"] for v in kt.values()))},
+        "roofline": rl,
         "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
         "gpu_launches": n_launch,
         "mixed": mixed,
@@ -554,9 +615,75 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def compare_forms(args):
+    """The FP64 form (the reference's arithmetic and Jacobi(3)-BiCGStab) and
+    DALM_MIXED (FP32 stencil fields, FP64 iterative refinement with
+    multigrid-CG FP32 inner solves) from the same seeded initial state for the
+    same steps: each turbine's power averaged over steps avg-from..STEPS in
+    both forms and their relative difference (the running average of
+    src/solver.h:1195-1204 applied to the loads of src/alm.h:384-398), the
+    final relative L2 differences of u, v, w and p, each form's largest
+    pressure residual and wall time.  The flow is chaotic: step-wise fields
+    drift apart from the solver-tolerance level; averages are what the two
+    forms must agree on."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    pkg = importlib.import_module("3dalm_b200")
+    tmp = tempfile.mkdtemp(prefix="dalm_compare_")
+    spec, mesh, U0, prof = make_case(args.case, tmp)
+    steps, avg_from = args.compare_forms, args.avg_from
+
+    def run(precision):
+        s = pkg.Solver(tmp, precision=precision, time_average=False)
+        if prof is not None:
+            s.set_inflow_profile(prof)
+        s.set_state(U0)
+        s.synchronize()
+        power, worst, its = None, 0.0, []
+        t = time.perf_counter()
+        s.step(1)  # step 0: no integration
+        for n in range(1, steps + 1):
+            s.step(1)
+            st = s.stats()
+            worst = max(worst, st["err"])
+            its.append(st["it"])
+            if n >= avg_from:
+                pw = s.turbines()[2]
+                power = pw.copy() if power is None else power + pw
+        s.synchronize()
+        wall = time.perf_counter() - t
+        out = {"power": power / (steps - avg_from + 1), "U": s.field("U"), "p": s.field("p"),
+               "turbines": s.turbines(), "max_residual": worst, "seconds": wall,
+               "iterations": its, "mesh": s.mesh(), "gc": s.gc}
+        s.finalize()
+        return out
+
+    with quiet_stdout():
+        f = run(pkg.FP64)
+        m = run(pkg.MIXED)
+    err = mixed_errors(m, f, f["mesh"], f["gc"])
+    out = {"workload": workload_config(args.case, spec.n[0] * spec.n[1] * spec.n[2], None, 1)[
+               "workload"], "case": args.case, "cells": list(spec.n), "steps": steps,
+           "dt": spec.dt, "average_over": [avg_from, steps], "tolerance": spec.tol,
+           "mean_power_fp64": f["power"].tolist(), "mean_power_mixed": m["power"].tolist(),
+           "mean_power_rel_diff": (np.abs(m["power"] - f["power"]) / np.abs(f["power"])).tolist(),
+           "final_rel_l2": err,
+           "max_residual_fp64": f["max_residual"], "max_residual_mixed": m["max_residual"],
+           "seconds_fp64": f["seconds"], "seconds_mixed": m["seconds"],
+           "speedup": f["seconds"] / m["seconds"],
+           "iterations_fp64_mean": float(np.mean(f["iterations"])),
+           "iterations_mixed_mean": float(np.mean(m["iterations"])),
+           "how": "wall time of each run including one host statistics call per step"}
+    print(json.dumps(out), flush=True)
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.compare_forms > 0:
+        compare_forms(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -124,3 +124,58 @@ def test_multigrid_inner_solves(make_case):
     assert kt["mg_pcg"]["launches"] > 0
     assert kt["bicg_xr32"]["launches"] == 0 and kt["jacobi_sweep32"]["launches"] == 0
     assert sum(its_m) * 5 <= sum(its_f)
+
+
+def is_fp32(v):
+    return np.array_equal(v, v.astype(np.float32).astype(np.float64))
+
+
+def test_mixed_stencil_fields_are_fp32(make_case):
+    """DALM_MIXED stores the stencil fields U (both time levels), JU and f in
+    FP32 and keeps p in FP64: every U, Uold, JU and f value the ABI returns
+    is an FP32 number, p is not; the flow kernels' algorithmic bytes are
+    those of 4-byte stencil fields."""
+    pkg = package()
+    spec, s, _ = setup(make_case, "tiny-loglaw", pkg.MIXED, with_oracle=False, profile=True)
+    s.step(4)
+    for f in ("U", "Uold", "JU", "f"):
+        v = s.field(f)
+        assert np.all(np.isfinite(v)) and np.any(v != 0), f
+        assert is_fp32(v), f"{f} is not stored in FP32"
+    assert not is_fp32(s.field("p"))
+    kt = s.kernel_timings()
+    cells = int(np.prod([n - 2 * s.gc for n in s.size]))
+    assert kt["project"]["bytes_per_launch"] == (12 * 4 + 8) * cells
+    assert kt["flux_rhs"]["bytes_per_launch"] == (6 * 4 + 8) * cells
+    assert kt["mg_smooth"]["bytes_per_launch"] > 0 and kt["mg_pcg"]["bytes_per_launch"] > 0
+
+
+def test_mixed_fp32_fields_set_and_step(make_case):
+    """Setting a field through the ABI rounds it into the FP32 field the
+    stages use; stepping from a state set that way equals stepping a solver
+    whose state was set identically (deterministic FP32 stages)."""
+    pkg = package()
+    spec, a, _ = setup(make_case, "tiny-turbine", pkg.MIXED, with_oracle=False)
+    _, b, _ = setup(make_case, "tiny-turbine", pkg.MIXED, with_oracle=False)
+    U = a.field("U")
+    rng = np.random.default_rng(3)
+    U2 = U + 1e-3 * rng.standard_normal(U.shape)
+    for x in (a, b):
+        x.set_state(U2)
+    got = a.field("U")
+    assert is_fp32(got)
+    gc = a.gc
+    inner = (slice(gc, -gc), slice(gc, -gc), slice(gc, -gc))
+    np.testing.assert_array_equal(got[inner], U2[inner].astype(np.float32).astype(np.float64))
+    a.step(3)
+    b.step(3)
+    for f in ("U", "p", "JU"):
+        np.testing.assert_array_equal(a.field(f), b.field(f))
+    np.testing.assert_array_equal(a.turbines()[0], b.turbines()[0])
+
+
+def test_mixed_adjoint_is_refused(make_case):
+    pkg = package()
+    spec, s, _ = setup(make_case, "tiny-turbine", pkg.MIXED, with_oracle=False)
+    with pytest.raises(pkg.DalmError):
+        s.power_gradient(1, 2, 1)
