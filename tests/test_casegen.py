@@ -82,12 +82,3 @@ def test_command_line_time_step(tmp_path):
     text = json.dumps(setup)
     assert '"dt": 0.0005' in text
     assert math.isclose(setup["runtime"]["time"], 3 * 5e-4)
-
-
-def test_timeline_kernel_names():
-    import importlib
-    tl = importlib.import_module("3dalm_b200.timeline")
-    assert tl.kernel_name("void dalm::(anonymous namespace)::k_mg_smooth<4, true, true>(x)") \
-        == "k_mg_smooth"
-    assert tl.kernel_name("void dalm::(anonymous namespace)::k_stencil<3>(a)") == "k_stencil<3>"
-    assert tl.kernel_name("k_project(dalm::StepParams)") == "k_project"
