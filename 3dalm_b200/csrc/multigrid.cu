@@ -4,6 +4,7 @@
 // device; every kernel returns at once once the solve is done, so batches
 // of iterations can be enqueued (and replayed as CUDA graphs) ahead of the
 // host's convergence check.
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -277,129 +278,218 @@ struct ZlineArgs {
     MgLevel C;
 };
 
-template <int R, bool FAC, bool VEC>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const KrylovState *st) {
-    __shared__ float slab[MG_THREADS / 32][33 * R];
+// The operands of one column's right-hand side in the VEC layout: f and the
+// four x/y neighbours' x of this lane's R rows.
+template <int R>
+struct ColumnLoads {
+    float f[R], e[R], w[R], n[R], s[R];
+};
+
+// Column `col` of the half-sweep's colour: (i, j), false past the grid.
+__device__ __forceinline__ bool zline_column(const MgLevel &L, unsigned col, unsigned njh, int color,
+                                             int &i, int &j) {
+    i = (int)(col / njh);
+    j = 2 * (int)(col - (unsigned)i * njh) + ((i + color) & 1);
+    return j < L.n[1];
+}
+
+template <int R>
+__device__ __forceinline__ void zline_load(const MgLevel &L, const float *x, const float *f, int i,
+                                           int j, int lane, ColumnLoads<R> &v) {
+    const long long c0 = L.at(i, j, 0) + R * lane;
+    load_seg<R>(f + c0, v.f);
+    load_seg<R>(x + c0 + L.g.sx, v.e);
+    load_seg<R>(x + c0 - L.g.sx, v.w);
+    load_seg<R>(x + c0 + L.g.sy, v.n);
+    load_seg<R>(x + c0 - L.g.sy, v.s);
+}
+
+// The VEC half-sweep without a pending prolongation (all but the first
+// half-sweep after a coarse correction), software-pipelined over the
+// columns a warp takes: the next column's operands are loaded before the
+// current column is solved, so their latency overlaps the line solve.  Same
+// arithmetic as k_mg_smooth's VEC path.
+template <int R, bool FAC>
+__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pipe(ZlineArgs A, const KrylovState *st) {
     if (st->done) return;
     const MgLevel &L = A.L;
     float *__restrict__ x = A.x;
     const float *__restrict__ f = A.f;
-    const float *__restrict__ xc = A.xc;
     const int lane = threadIdx.x & 31;
-    float *sl = slab[threadIdx.x >> 5];
-    // column n of the colour: i = n / njh, j = 2 (n % njh) + (i + color) % 2
     const unsigned njh = (unsigned)(L.n[1] + 1) / 2;
     const unsigned ncol = (unsigned)L.n[0] * njh;
     const unsigned nw = gridDim.x * (blockDim.x >> 5);
     const int nk = L.n[2];
     const bool zero = A.zero_start != 0;
-    const int kshift = A.C.fac[2] == 2 ? 1 : 0;
-    for (unsigned col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); col < ncol;
-         col += nw) {
-        const int i = (int)(col / njh);
-        const int j = 2 * (int)(col - (unsigned)i * njh) + ((i + A.color) & 1);
-        if (j >= L.n[1]) continue;  // uniform in the warp
-        const long long c0 = L.at(i, j, 0);
-        // parents of the interior x and y neighbours (-1: boundary, no correction)
-        long long pe = -1, pw = -1, pn = -1, ps = -1;
-        if (xc) {
-            const MgLevel &C = A.C;
-            const int I = i / C.fac[0], J = j / C.fac[1];
-            if (i + 1 < L.n[0]) pe = C.at((i + 1) / C.fac[0], J, 0);
-            if (i > 0) pw = C.at((i - 1) / C.fac[0], J, 0);
-            if (j + 1 < L.n[1]) pn = C.at(I, (j + 1) / C.fac[1], 0);
-            if (j > 0) ps = C.at(I, (j - 1) / C.fac[1], 0);
-        }
-        // the column's constants (mg_zline_coef and mg_zline_rhs per row)
-        const float wi = L.w[0][i], wj = L.w[1][j];
-        const float xe = L.cf[0][i + 1], xw = L.cf[0][i], yn = L.cf[1][j + 1], ys = L.cf[1][j];
-        const float az = wi * wj, sxy = wj * (xe + xw) + wi * (yn + ys);
-        const float *w2 = L.w[2], *cf2 = L.cf[2];
-        // the column and its x and y neighbours, from k = 0
-        const float *fr = f + c0, *xre = x + c0 + L.g.sx, *xrw = x + c0 - L.g.sx,
-                    *xrn = x + c0 + L.g.sy, *xrs = x + c0 - L.g.sy;
-        float d[R], xs[R];
-        if (VEC) {
-            // this lane's rows k = R lane + s, with vector loads
-            const int k0 = R * lane;
-            float vf[R], vw2[R], ve[R], vw[R], vn[R], vs[R];
-            load_seg<R>(fr + k0, vf);
-            if (!zero) {
-                load_seg<R>(w2 + k0, vw2);
-                load_seg<R>(xre + k0, ve);
-                load_seg<R>(xrw + k0, vw);
-                load_seg<R>(xrn + k0, vn);
-                load_seg<R>(xrs + k0, vs);
-                if (xc) {
-#pragma unroll
-                    for (int q = 0; q < R; q++) {
-                        const int K = (k0 + q) >> kshift;
-                        if (pe >= 0) ve[q] += xc[pe + K];
-                        if (pw >= 0) vw[q] += xc[pw + K];
-                        if (pn >= 0) vn[q] += xc[pn + K];
-                        if (ps >= 0) vs[q] += xc[ps + K];
-                    }
-                }
-            }
+    const float *w2 = L.w[2], *cf2 = L.cf[2];
+    float vw2[R];
+    load_seg<R>(w2 + R * lane, vw2);
+    unsigned col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int i = 0, j = 0;
+    bool ok = col < ncol && zline_column(L, col, njh, A.color, i, j);
+    ColumnLoads<R> cur, nxt;
+    if (ok) zline_load<R>(L, x, f, i, j, lane, cur);
+    while (col < ncol) {
+        const unsigned ncol2 = col + nw;
+        int i2 = 0, j2 = 0;
+        const bool ok2 = ncol2 < ncol && zline_column(L, ncol2, njh, A.color, i2, j2);
+        if (ok2) zline_load<R>(L, x, f, i2, j2, lane, nxt);
+        if (ok) {
+            const float wi = L.w[0][i], wj = L.w[1][j];
+            const float xe = L.cf[0][i + 1], xw = L.cf[0][i], yn = L.cf[1][j + 1], ys = L.cf[1][j];
+            float d[R], xs[R];
 #pragma unroll
             for (int q = 0; q < R; q++)
-                d[q] = zero ? vf[q]
-                            : vf[q] + vw2[q] * (wj * (xe * ve[q] + xw * vw[q]) +
-                                                wi * (yn * vn[q] + ys * vs[q]));
-        } else {
-            // all of the column's loads first, then the slab
-            float rhs[R];
+                d[q] = zero ? cur.f[q]
+                            : cur.f[q] + vw2[q] * (wj * (xe * cur.e[q] + xw * cur.w[q]) +
+                                                   wi * (yn * cur.n[q] + ys * cur.s[q]));
+            if (FAC) {
+                line_solve_table<R>(L.ltab + (size_t)(L.lcls[0][i] * L.lky + L.lcls[1][j]) *
+                                                 mglf_count(R) * 32 + lane,
+                                    lane, d, xs);
+            } else {
+                const float az = wi * wj, sxy = wj * (xe + xw) + wi * (yn + ys);
+                line_solve<R>(az, sxy, w2, cf2, nk, lane, d, xs);
+            }
+            store_seg<R>(x + L.at(i, j, 0) + R * lane, xs);
+        }
+        col = ncol2;
+        i = i2;
+        j = j2;
+        ok = ok2;
+        cur = nxt;
+    }
+}
+
+// One column (i, j) of a zebra z-line half-sweep (see above); sl is the
+// warp's slab of 33 R floats (unused on the VEC path).
+template <int R, bool FAC, bool VEC>
+__device__ __forceinline__ void zline_solve_column(const ZlineArgs &A, int i, int j, int lane,
+                                                   float *sl) {
+    const MgLevel &L = A.L;
+    float *__restrict__ x = A.x;
+    const float *__restrict__ f = A.f;
+    const float *__restrict__ xc = A.xc;
+    const int nk = L.n[2];
+    const bool zero = A.zero_start != 0;
+    const int kshift = A.C.fac[2] == 2 ? 1 : 0;
+    const long long c0 = L.at(i, j, 0);
+    // parents of the interior x and y neighbours (-1: boundary, no correction)
+    long long pe = -1, pw = -1, pn = -1, ps = -1;
+    if (xc) {
+        const MgLevel &C = A.C;
+        const int I = i / C.fac[0], J = j / C.fac[1];
+        if (i + 1 < L.n[0]) pe = C.at((i + 1) / C.fac[0], J, 0);
+        if (i > 0) pw = C.at((i - 1) / C.fac[0], J, 0);
+        if (j + 1 < L.n[1]) pn = C.at(I, (j + 1) / C.fac[1], 0);
+        if (j > 0) ps = C.at(I, (j - 1) / C.fac[1], 0);
+    }
+    // the column's constants (mg_zline_coef and mg_zline_rhs per row)
+    const float wi = L.w[0][i], wj = L.w[1][j];
+    const float xe = L.cf[0][i + 1], xw = L.cf[0][i], yn = L.cf[1][j + 1], ys = L.cf[1][j];
+    const float az = wi * wj, sxy = wj * (xe + xw) + wi * (yn + ys);
+    const float *w2 = L.w[2], *cf2 = L.cf[2];
+    // the column and its x and y neighbours, from k = 0
+    const float *fr = f + c0, *xre = x + c0 + L.g.sx, *xrw = x + c0 - L.g.sx,
+                *xrn = x + c0 + L.g.sy, *xrs = x + c0 - L.g.sy;
+    float d[R], xs[R];
+    if (VEC) {
+        // this lane's rows k = R lane + s, with vector loads
+        const int k0 = R * lane;
+        float vf[R], vw2[R], ve[R], vw[R], vn[R], vs[R];
+        load_seg<R>(fr + k0, vf);
+        if (!zero) {
+            load_seg<R>(w2 + k0, vw2);
+            load_seg<R>(xre + k0, ve);
+            load_seg<R>(xrw + k0, vw);
+            load_seg<R>(xrn + k0, vn);
+            load_seg<R>(xrs + k0, vs);
+            if (xc) {
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                const int k = lane + 32 * r;
-                rhs[r] = 0.f;
-                if (k < nk) {
-                    rhs[r] = fr[k];
-                    if (!zero) {
-                        float ve = xre[k], vw = xrw[k], vn = xrn[k], vs = xrs[k];
-                        if (xc) {
-                            const int K = k >> kshift;
-                            if (pe >= 0) ve += xc[pe + K];
-                            if (pw >= 0) vw += xc[pw + K];
-                            if (pn >= 0) vn += xc[pn + K];
-                            if (ps >= 0) vs += xc[ps + K];
-                        }
-                        rhs[r] += w2[k] * (wj * (xe * ve + xw * vw) + wi * (yn * vn + ys * vs));
-                    }
+                for (int q = 0; q < R; q++) {
+                    const int K = (k0 + q) >> kshift;
+                    if (pe >= 0) ve[q] += xc[pe + K];
+                    if (pw >= 0) vw[q] += xc[pw + K];
+                    if (pn >= 0) vn[q] += xc[pn + K];
+                    if (ps >= 0) vs[q] += xc[ps + K];
                 }
             }
-            __syncwarp();  // the previous column's reads of the slab are done
+        }
 #pragma unroll
-            for (int r = 0; r < R; r++) sl[lane + 33 * r] = rhs[r];
-            __syncwarp();
+        for (int q = 0; q < R; q++)
+            d[q] = zero ? vf[q]
+                        : vf[q] + vw2[q] * (wj * (xe * ve[q] + xw * vw[q]) +
+                                            wi * (yn * vn[q] + ys * vs[q]));
+    } else {
+        // all of the column's loads first, then the slab
+        float rhs[R];
 #pragma unroll
-            for (int s = 0; s < R; s++) {
-                const int k = R * lane + s;
-                d[s] = sl[k + (k >> 5)];
+        for (int r = 0; r < R; r++) {
+            const int k = lane + 32 * r;
+            rhs[r] = 0.f;
+            if (k < nk) {
+                rhs[r] = fr[k];
+                if (!zero) {
+                    float ve = xre[k], vw = xrw[k], vn = xrn[k], vs = xrs[k];
+                    if (xc) {
+                        const int K = k >> kshift;
+                        if (pe >= 0) ve += xc[pe + K];
+                        if (pw >= 0) vw += xc[pw + K];
+                        if (pn >= 0) vn += xc[pn + K];
+                        if (ps >= 0) vs += xc[ps + K];
+                    }
+                    rhs[r] += w2[k] * (wj * (xe * ve + xw * vw) + wi * (yn * vn + ys * vs));
+                }
             }
         }
-        if (FAC)
-            line_solve_table<R>(L.ltab + (size_t)(L.lcls[0][i] * L.lky + L.lcls[1][j]) *
-                                             mglf_count(R) * 32 + lane,
-                                lane, d, xs);
-        else
-            line_solve<R>(az, sxy, w2, cf2, nk, lane, d, xs);
-        // 4. store (through the slab into the coalesced layout unless VEC)
-        if (VEC) {
-            store_seg<R>(x + c0 + R * lane, xs);
-        } else {
+        __syncwarp();  // the previous column's reads of the slab are done
 #pragma unroll
-            for (int s = 0; s < R; s++) {
-                const int k = R * lane + s;
-                sl[k + (k >> 5)] = xs[s];
-            }
-            __syncwarp();
+        for (int r = 0; r < R; r++) sl[lane + 33 * r] = rhs[r];
+        __syncwarp();
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                const int k = lane + 32 * r;
-                if (k < nk) x[c0 + k] = sl[k + r];
-            }
+        for (int s = 0; s < R; s++) {
+            const int k = R * lane + s;
+            d[s] = sl[k + (k >> 5)];
         }
+    }
+    if (FAC)
+        line_solve_table<R>(L.ltab + (size_t)(L.lcls[0][i] * L.lky + L.lcls[1][j]) *
+                                         mglf_count(R) * 32 + lane,
+                            lane, d, xs);
+    else
+        line_solve<R>(az, sxy, w2, cf2, nk, lane, d, xs);
+    // 4. store (through the slab into the coalesced layout unless VEC)
+    if (VEC) {
+        store_seg<R>(x + c0 + R * lane, xs);
+    } else {
+#pragma unroll
+        for (int s = 0; s < R; s++) {
+            const int k = R * lane + s;
+            sl[k + (k >> 5)] = xs[s];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int k = lane + 32 * r;
+            if (k < nk) x[c0 + k] = sl[k + r];
+        }
+    }
+}
+
+template <int R, bool FAC, bool VEC>
+__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const KrylovState *st) {
+    __shared__ float slab[MG_THREADS / 32][33 * R];
+    if (st->done) return;
+    const int lane = threadIdx.x & 31;
+    float *sl = slab[threadIdx.x >> 5];
+    const unsigned njh = (unsigned)(A.L.n[1] + 1) / 2;
+    const unsigned ncol = (unsigned)A.L.n[0] * njh;
+    const unsigned nw = gridDim.x * (blockDim.x >> 5);
+    for (unsigned col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); col < ncol;
+         col += nw) {
+        int i, j;
+        if (!zline_column(A.L, col, njh, A.color, i, j)) continue;  // uniform in the warp
+        zline_solve_column<R, FAC, VEC>(A, i, j, lane, sl);
     }
 }
 
@@ -421,7 +511,11 @@ bool zline_vec_ok(const ZlineArgs &a, int R) {
 template <int R>
 void zline_launch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st, int blocks) {
     const bool vec = zline_vec_ok(a, R);
-    if (a.L.ltab && vec)
+    if (vec && !a.xc && a.L.ltab)
+        k_mg_smooth_pipe<R, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+    else if (vec && !a.xc)
+        k_mg_smooth_pipe<R, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+    else if (a.L.ltab && vec)
         k_mg_smooth<R, true, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
     else if (a.L.ltab)
         k_mg_smooth<R, true, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
@@ -451,21 +545,19 @@ void zline_dispatch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *s
 
 // coarse cell (I,J,K) = the sum of its children's residuals f - K x,
 // leaving out the children of colour `skip` (as mg_restrict_sum).  One warp
-// per coarse row, U coarse cells per lane at a time: the child rows (at most
-// 2 x 2, levels merge at most two cells per axis) are visited one after the
-// other, each with its row constants, and the sums are stored at the end.
-__global__ void __launch_bounds__(MG_THREADS)
-k_mg_restrict(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, int skip,
-              const KrylovState *st) {
-    if (st->done) return;
+// per coarse row (warps w0, w0 + nw, ...), U coarse cells per lane at a
+// time: the child rows (at most 2 x 2, levels merge at most two cells per
+// axis) are visited one after the other, each with its row constants, and
+// the sums are stored at the end.
+__device__ __forceinline__ void mg_restrict_rows(const MgLevel &F, const MgLevel &C, const float *x,
+                                                 const float *f, float *fc, int skip, unsigned w0,
+                                                 unsigned nw) {
     constexpr int U = 4;
     const int lane = threadIdx.x & 31;
     const int nk = C.n[2], f2 = C.fac[2];
     const unsigned nj = (unsigned)C.n[1];
     const unsigned rows = (unsigned)C.n[0] * nj;
-    const unsigned nw = gridDim.x * (blockDim.x >> 5);
-    for (unsigned row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < rows;
-         row += nw) {
+    for (unsigned row = w0; row < rows; row += nw) {
         const int I = (int)(row / nj), J = (int)(row - (unsigned)I * nj);
         const long long cc = C.at(I, J, 0);
         for (int k0 = 0; k0 < nk; k0 += 32 * U) {
@@ -496,14 +588,19 @@ k_mg_restrict(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, i
     }
 }
 
-// x = K^-1 f on the coarsest level: one warp per row of the dense inverse
 __global__ void __launch_bounds__(MG_THREADS)
-k_mg_coarse(MgLevel C, const float *kinv, int n, const float *f, float *x,
-            const KrylovState *st) {
+k_mg_restrict(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, int skip,
+              const KrylovState *st) {
     if (st->done) return;
+    mg_restrict_rows(F, C, x, f, fc, skip, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5),
+                     gridDim.x * (blockDim.x >> 5));
+}
+
+// x = K^-1 f on the coarsest level: one warp per row of the dense inverse
+__device__ __forceinline__ void mg_coarse_rows(const MgLevel &C, const float *kinv, int n,
+                                               const float *f, float *x, int w0, int nw) {
     const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n; r += warps) {
+    for (int r = w0; r < n; r += nw) {
         const float *row = kinv + (long long)r * n;
         float s = 0;
         for (int c = lane; c < n; c += 32) s += row[c] * f[mg_cell_index(C, c)];
@@ -511,6 +608,14 @@ k_mg_coarse(MgLevel C, const float *kinv, int n, const float *f, float *x,
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) x[mg_cell_index(C, r)] = s;
     }
+}
+
+__global__ void __launch_bounds__(MG_THREADS)
+k_mg_coarse(MgLevel C, const float *kinv, int n, const float *f, float *x,
+            const KrylovState *st) {
+    if (st->done) return;
+    mg_coarse_rows(C, kinv, n, f, x, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5),
+                   gridDim.x * (blockDim.x >> 5));
 }
 
 // f = -max_diag vol r (in place), e = 0

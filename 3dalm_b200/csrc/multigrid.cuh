@@ -245,7 +245,7 @@ void mg_vcycle(E &e, int levels, int nu) {
 // conjugate-gradient iterations per step where 2 everywhere gives 5-7, at
 // 0.86x the step time)
 constexpr int MG_NU = 2;
-inline int mg_nu(int level) { return level == 0 ? 4 : level == 1 ? 3 : MG_NU; }
+DALM_HD int mg_nu(int level) { return level == 0 ? 4 : level == 1 ? 3 : MG_NU; }
 
 // Device state of the preconditioner (multigrid.cu).
 struct MgDev {

@@ -343,12 +343,12 @@ void fused_launch(const LaunchCtx &L, int kind_tag, const Grid &g, const Poisson
                   const PoissonConfig &cfg, const CUtensorMap &ma, const CUtensorMap &mb,
                   const CUtensorMap &mc, const CUtensorMap &mr0, const FusedArgs &A,
                   Partials<2> part, KrylovState *st) {
-    static bool configured = false;  // per process; the attribute is per function
-    if (!configured) {
-        DALM_CUDA(cudaFuncSetAttribute(k_fused<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       FusedGeo<KIND>::SMEM));
-        configured = true;
-    }
+    // The shared-memory limit is an attribute of the function in the current
+    // device's context: set it on every launch (a host-side call of about a
+    // microsecond), so handles on several devices or threads need no shared
+    // flag.
+    DALM_CUDA(cudaFuncSetAttribute(k_fused<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   FusedGeo<KIND>::SMEM));
     L.pre(kind_tag);
     k_fused<KIND><<<cfg.seg.count, TILE_THREADS, FusedGeo<KIND>::SMEM, L.s>>>(
         g, C, cfg.seg, ma, mb, mc, mr0, A, part, st);
