@@ -1,24 +1,32 @@
 #!/usr/bin/env python
 """Benchmark of the 3dalm time step on one B200 per rank.
 
-Workload: the 3-turbine case, 512x256x128 interior cells (16.78 M) over a
-20x5x5 domain stretched toward the ground, turbines at x = 4, 9, 14 (yaw 0,
-10, 0 deg, 3 blades x 32 points, R = 0.5, TSR 6), log-law inflow
-(u* = 0.05, z0 = 1e-3) + seeded 8% Gaussian perturbation, Re = 1e4,
-Cs = 0.1, dt = 1e-3, minmod MUSCL, Jacobi(3)-preconditioned BiCGStab to
-1e-8.  Synthetic inputs (no dataset exists for this solver); every field is
-larger than the 126 MB L2, so no L2 flush is needed between steps.
+Workload (default --case c4): the 3-turbine case, 512x256x128 interior
+cells (16.78 M) over a 20x5x5 domain stretched toward the ground, turbines
+at x = 4, 9, 14 (yaw 0, 10, 0 deg, 3 blades x 32 points, R = 0.5, TSR 6),
+log-law inflow (u* = 0.05, z0 = 1e-3) + seeded 8% Gaussian perturbation,
+Re = 1e4, Cs = 0.1, minmod MUSCL, Jacobi(3)-preconditioned BiCGStab to 1e-8,
+dt = 5e-4 (BENCH_DT).  Synthetic inputs (no dataset exists for this
+solver); every field is larger than the 126 MB L2, so no L2 flush is
+needed between steps.
 
 A step is Solver::main_loop_once: predictor, face flux + Poisson RHS, the
 Poisson solve to tolerance, projection + BCs, actuator line.  Metric:
 Mcell-steps/s = interior cells x steps / time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --compare-forms STEPS     (FP64 vs mixed over a long run)
 
 The headline `value` is the reference's precision (FP64).  The line also
-carries `mixed`: the same timed steps with DALM_MIXED (FP64 iterative
-refinement with capped FP32 BiCGStab passes), its ratio to FP64 and both
-forms' largest final FP64 residual.
+carries `mixed`: the same timed steps with DALM_MIXED (FP32 stencil fields;
+FP64 iterative refinement with FP32 multigrid-preconditioned CG inner
+solves), its ratio to the FP64 form, its roofline, both forms' largest
+final FP64 residual and its per-field / per-turbine errors against the FP64
+form; and `e2e`, `roofline`, `cpu_baseline`, `clocks`, `adjoint`.
+
+--impl reference runs the reference's own CPU step (oracle/_ref/ref_mpirun:
+its sources compiled with OpenACC off, as MPI ranks on every host core) on
+the same case and steps, whole steps within a wall budget.
 
 With N > 1 (torchrun) every rank runs an independent replica of the case on
 its own GPU (the path has no exchange step on one domain): weak scaling, no
@@ -52,16 +60,33 @@ CASE = "c4"
 # stably (max CFL 0.08 falling to 0.02 over 60 steps).
 BENCH_DT = 5e-4
 
+def workload_description(case):
+    """One line naming the case's grid, rotor count, solver and inflow."""
+    cg = importlib.import_module("3dalm_b200.casegen")
+    spec = cg.config(case)
+    n = "x".join(str(v) for v in spec.n)
+    solver = {"SOR": f"red-black SOR w={spec.relax} to {spec.tol:g}",
+              "BiCG": f"{spec.pc}({spec.pc_max_it})-BiCGStab to {spec.tol:g}",
+              "Jacobi": f"Jacobi to {spec.tol:g}"}[spec.solver]
+    inflow = (f"log-law inflow + {spec.intensity:.0%} noise" if spec.loglaw
+              else f"uniform inflow + {spec.intensity:.0%} noise")
+    rotors = len(spec.turbines)
+    pts = rotors * spec.blades * spec.points_per_blade
+    what = f"{rotors}-turbine" if rotors else "no-turbine"
+    tail = f", {pts} blade points" if rotors else ""
+    return f"{what} {n} LES step ({solver}, {inflow}{tail})"
+
+
 def workload_config(case, cells, iterations, world, dt=BENCH_DT):
     """The `config` object both arms report."""
-    return {"workload": "3-turbine 512x256x128 LES step (Jacobi(3)-BiCGStab to 1e-8, log-law "
-                        "inflow + 8% noise, 288 blade points)",
+    return {"workload": workload_description(case),
             "case": case, "dt": dt,
-            "dt_note": "configured 1e-3 diverges in the reference's explicit scheme "
-                       "(wall-cell diffusion instability); see BENCH_DT in bench.py",
+            "dt_note": "configured 1e-3 diverges in the reference's explicit scheme on the "
+                       "128-cell stretched z columns (wall-cell diffusion instability); see "
+                       "BENCH_DT in bench.py",
             "precision": "FP64", "cells": cells,
             "poisson_iterations": iterations, "parallelism": f"replicas x{world}",
-            "l2": "every field > 126 MB L2 (134 MB per scalar field); no flush"}
+            "l2": "every field > 126 MB L2 (134 MB per scalar field at 512x256x128); no flush"}
 
 
 @contextlib.contextmanager
@@ -305,18 +330,18 @@ def run_reference_ranks(case, warmup, steps, ranks, max_it=None, budget=0.0, tim
     return res
 
 
-def reference_sample(ranks, iterations):
+def reference_sample(ranks, iterations, case=CASE):
     """cpu_baseline: a bounded sample of the benchmark workload on the host
     cores: one whole step (step 1 from the seeded initial state) of the full
     512x256x128 case through the reference's own code as `ranks` MPI ranks,
     with its pressure solve capped at the GPU arm's mean iteration count of
     the timed steps (so the sample does the same work per step as they do)."""
     it = max(1, int(round(iterations)))
-    res = run_reference_ranks(CASE, 1, 1, ranks, max_it=it)
+    res = run_reference_ranks(case, 1, 1, ranks, max_it=it)
     secs = res["seconds"]
     desc = (f"reference (oracle/_ref/ref_mpirun: the reference's own step, OpenACC off) as "
             f"{ranks} MPI ranks on {ranks} host cores; one whole step of the same "
-            f"512x256x128 case (step 1 from the seeded initial state) with the pressure "
+            f"case (step 1 from the seeded initial state) with the pressure "
             f"solve capped at {it} iterations, the GPU arm's mean over its timed steps "
             f"(ran {res['iterations'][0]})")
     return res["cells"] / secs / 1e6, "reference", desc, secs
@@ -604,7 +629,7 @@ def run_ours(args):
         line["adjoint"] = adjoint_cost(pkg, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_MPIRUN):
         ranks = host_cores()
-        v, kind, desc, secs = reference_sample(ranks, statistics.mean(its))
+        v, kind, desc, secs = reference_sample(ranks, statistics.mean(its), args.case)
         line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": ranks, "kind": kind,
                                 "sample": desc, "sample_seconds": secs}
     s.finalize()
@@ -663,8 +688,7 @@ def compare_forms(args):
         f = run(pkg.FP64)
         m = run(pkg.MIXED)
     err = mixed_errors(m, f, f["mesh"], f["gc"])
-    out = {"workload": workload_config(args.case, spec.n[0] * spec.n[1] * spec.n[2], None, 1)[
-               "workload"], "case": args.case, "cells": list(spec.n), "steps": steps,
+    out = {"workload": workload_description(args.case), "case": args.case, "cells": list(spec.n), "steps": steps,
            "dt": spec.dt, "average_over": [avg_from, steps], "tolerance": spec.tol,
            "mean_power_fp64": f["power"].tolist(), "mean_power_mixed": m["power"].tolist(),
            "mean_power_rel_diff": (np.abs(m["power"] - f["power"]) / np.abs(f["power"])).tolist(),

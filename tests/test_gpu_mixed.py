@@ -179,3 +179,56 @@ def test_mixed_adjoint_is_refused(make_case):
     spec, s, _ = setup(make_case, "tiny-turbine", pkg.MIXED, with_oracle=False)
     with pytest.raises(pkg.DalmError):
         s.power_gradient(1, 2, 1)
+
+
+TGG_BICG = dict(solver="BiCG", pc="Jacobi", pc_max_it=3, tol=1e-8, max_it=2000)
+
+
+def test_mixed_with_grid_floor_and_probes(make_case):
+    """The FP32 stencil fields carry the turbulence-generating grid (solid
+    scaling in the projection), the retracted floor (slip rows of the
+    velocity BCs) and the probes: a BiCGStab version of the grid case stays
+    within the mixed envelope of the FP64 oracle over ten steps."""
+    pkg = package()
+    spec, mesh, d, U0, prof = make_case("tiny-tgg", **TGG_BICG)
+    s = pkg.Solver(d, precision=pkg.MIXED)
+    o = O.CRestatement(d)
+    for x in (s, o):
+        x.set_state(U0)
+    worst = 0.0
+    for n in range(11):
+        s.step(1)
+        o.step(1)
+        if n >= 1:
+            assert s.stats()["err"] <= spec.tol
+        U, Uo = s.field("U"), o.field("U")
+        for m in range(3):
+            worst = max(worst, rel(U[..., m], Uo[..., m]))
+    assert is_fp32(s.field("U"))
+    assert worst <= MIXED_ENVELOPE["U"], worst
+
+
+def test_mixed_output_files(make_case):
+    """With write_output the mixed form writes the reference's files from
+    its FP32 fields: the inst_ velocity is FP32-valued and close to the FP64
+    form's at the same step."""
+    import os
+    from test_gpu_output import read_binary
+    pkg = package()
+    out = dict(output_start_time=0.0, output_interval_time=0.002, tavg_start_time=0.003)
+    spec, mesh, d, U0, prof = make_case("tiny-turbine", steps=4, **out)
+    files = {}
+    for prec in (pkg.MIXED, pkg.FP64):
+        s = pkg.Solver(d, precision=prec, write_output=True)
+        s.set_state(U0)
+        s.step(spec.steps + 1)
+        s.finalize()
+        odir = os.path.join(d, "output")
+        names = sorted(n for n in os.listdir(odir) if n.startswith("inst_"))
+        assert names, "no inst_ files written"
+        files[prec] = read_binary(os.path.join(odir, names[-1]))[4]
+        for n in os.listdir(odir):
+            os.remove(os.path.join(odir, n))
+    um, uf = files[pkg.MIXED]["U"], files[pkg.FP64]["U"]
+    assert is_fp32(um)
+    assert np.linalg.norm(um - uf) / np.linalg.norm(uf) <= 1e-6
