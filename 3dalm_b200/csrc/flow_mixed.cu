@@ -290,11 +290,6 @@ __global__ void __launch_bounds__(256) k_copy_guides32(Grid g, Vec3<const float>
     }
 }
 
-__device__ __forceinline__ bool interior(const Grid &g, int i, int j, int k) {
-    return i >= g.gc && i < g.nx - g.gc && j >= g.gc && j < g.ny - g.gc && k >= g.gc &&
-           k < g.nz - g.gc;
-}
-
 // Face flux with the apply_JUbc overrides (src/bc.h:235-302 and the inflow
 // profile extension); faces are named by their lower cell.  FP32.
 __device__ __forceinline__ float flux_x32(const StepParams &P, float u0, float u1, float yz, int i,

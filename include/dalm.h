@@ -41,16 +41,23 @@ extern "C" {
 /* ---- enums ------------------------------------------------------------ */
 enum dalm_precision {
     DALM_FP64 = 0,        /* every stage in FP64, the reference's arithmetic */
-    DALM_MIXED = 1        /* BiCGStab pressure solve by FP64 iterative
-                             refinement with FP32 inner passes
-                             (dalm_options.mixed_inner: multigrid-
-                             preconditioned CG by default, or the case's
-                             BiCGStab): residual, norms, dots and the
-                             pressure in FP64, the stop test on the FP64
-                             residual; a pass that stalls or breaks down
-                             hands the rest of the solve to the FP64
-                             solver.  Every other stage, and SOR / Jacobi
-                             solves, FP64.                               */
+    DALM_MIXED = 1        /* BiCGStab cases: the stencil fields U, JU and
+                             f stored and computed in FP32 (predictor,
+                             face fluxes, projection, velocity BCs), the
+                             pressure solve by FP64 iterative refinement
+                             with FP32 inner passes (dalm_options.
+                             mixed_inner: multigrid-preconditioned CG by
+                             default, or the case's BiCGStab); the
+                             pressure, the Poisson right-hand side, the
+                             pressure-gradient corrections, residuals,
+                             norms, dots and the blade-point model in
+                             FP64, the stop test on the FP64 residual; a
+                             pass that stalls or breaks down hands the
+                             rest of the solve to the FP64 solver.  With
+                             reference_sums the stencil fields stay FP64;
+                             SOR / Jacobi cases run in FP64.  The ABI
+                             reads and writes the fields in FP64 (values
+                             are rounded to FP32 on the way in).          */
 };
 
 enum dalm_limiter {
@@ -97,11 +104,12 @@ typedef struct dalm_handle dalm_handle;
  * refinement, whose stop test is the reference's. */
 enum dalm_mixed_inner {
     DALM_INNER_MULTIGRID = 0, /* conjugate gradients preconditioned by a
-                                 geometric multigrid V-cycle (red-black
-                                 Gauss-Seidel, piecewise-constant transfers,
-                                 exact coarsest solve); falls back to
+                                 geometric multigrid V-cycle (zebra z-line
+                                 relaxation with x-y semi-coarsening,
+                                 piecewise-constant transfers, exact
+                                 coarsest solve); falls back to
                                  DALM_INNER_BICGSTAB when the coarsest level
-                                 would exceed 1024 cells                   */
+                                 would exceed 1024 cells or a z-column 256 */
     DALM_INNER_BICGSTAB = 1   /* the case's Jacobi(k)-preconditioned BiCGStab
                                  (src/eq.h:333-402) in FP32 vectors        */
 };
@@ -119,9 +127,12 @@ typedef struct {
                              (dalm_get_kernel_timings)                   */
     int reference_sums;   /* 1: every global sum (Krylov dots, norms,
                              divergence norm) in the reference's serial
-                             cell order instead of a parallel tree; with it
-                             the FP64 step reproduces the reference's
-                             rounding (slow: for parity checks)          */
+                             cell order instead of a parallel tree, and
+                             the actuator line (blade points and the dense
+                             Gaussian projection) evaluated on the host
+                             with the host's libm; with it the FP64 step
+                             reproduces the reference's rounding, turbines
+                             included (slow: for parity checks)          */
     int fused_krylov;     /* 1: each half of a Jacobi(3)-BiCGStab
                              iteration (update, preconditioner, SpMV, dot
                              products) as one kernel, 20 instead of 35
