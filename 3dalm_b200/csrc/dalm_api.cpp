@@ -1164,6 +1164,9 @@ struct dalm_handle {
         std::filesystem::create_directories(out_dir);
         write_partition_json(out_dir + "/partition.json", cs.size, cs.gc);
         next_output_time = cs.output_start_time;
+        if (alm.ap_count > 0)  // the blade-point tables at set-up (src/solver.h:949-974)
+            write_ap_info(out_dir + "/ap_info.log", alm.ap_count, alm.atk_count, cs.ap_r,
+                          cs.ap_dr, cs.ap_chord, base_twist, cs.ap_cd, cs.ap_cl, cs.atk);
         if (alm.wt_count > 0) {
             turbine_log.open(out_dir + "/turbines.csv");
             if (!turbine_log) throw std::runtime_error("cannot write " + out_dir + "/turbines.csv");

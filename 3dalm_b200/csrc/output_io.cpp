@@ -88,4 +88,28 @@ void write_partition_json(const std::string &path, const int64_t size[3], int64_
       << "\n}";
 }
 
+void write_ap_info(const std::string &path, int64_t ap_count, int64_t atk_count,
+                   const std::vector<double> &r, const std::vector<double> &dr,
+                   const std::vector<double> &chord, const std::vector<double> &twist,
+                   const std::vector<double> &cd, const std::vector<double> &cl,
+                   const std::vector<double> &atk) {
+    FILE *f = std::fopen(path.c_str(), "w");
+    if (!f) throw std::runtime_error("cannot write " + path);
+    std::fprintf(f, "ap count = %ld, atk acount = %ld\n", (long)ap_count, (long)atk_count);
+    for (int64_t a = 0; a < ap_count; a++) {
+        std::fprintf(f, "ap %ld\n", (long)a);
+        std::fprintf(f, "\tr = %lf\n", r[a]);
+        std::fprintf(f, "\tdr = %lf\n", dr[a]);
+        std::fprintf(f, "\tchord = %lf\n", chord[a]);
+        std::fprintf(f, "\ttwist = %lf\n", twist[a]);
+        std::fprintf(f, "\tcd = \n");
+        for (int64_t j = 0; j < atk_count; j++) std::fprintf(f, "\t\t%lf\n", cd[a * atk_count + j]);
+        std::fprintf(f, "\tcl = \n");
+        for (int64_t j = 0; j < atk_count; j++) std::fprintf(f, "\t\t%lf\n", cl[a * atk_count + j]);
+    }
+    std::fprintf(f, "atk\n");
+    for (int64_t j = 0; j < atk_count; j++) std::fprintf(f, "\t%lf\n", atk[j]);
+    std::fclose(f);
+}
+
 }  // namespace dalm

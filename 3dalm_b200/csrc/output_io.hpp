@@ -38,4 +38,13 @@ void write_snapshot_json(const std::string &path, const std::vector<SnapshotEntr
 // partition.json of one rank holding the whole grid (src/solver.h:980-998)
 void write_partition_json(const std::string &path, const int64_t size[3], int64_t gc);
 
+// ap_info.log (src/solver.h:949-974): the blade-point tables after set-up,
+// per point r, dr, chord, twist and its Cd / Cl columns over the
+// angle-of-attack list ([ap][atk] row-major), then that list; "%lf" numbers.
+void write_ap_info(const std::string &path, int64_t ap_count, int64_t atk_count,
+                   const std::vector<double> &r, const std::vector<double> &dr,
+                   const std::vector<double> &chord, const std::vector<double> &twist,
+                   const std::vector<double> &cd, const std::vector<double> &cl,
+                   const std::vector<double> &atk);
+
 }  // namespace dalm
