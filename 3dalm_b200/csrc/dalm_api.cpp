@@ -847,21 +847,30 @@ struct dalm_handle {
         launch_poisson_begin(L, d_kst, max_it, tol, ncell, MAX_REFINE, INNER_RTOL, cap);
         launch_poisson_begin(L, d_kst + 1, max_it, tol, ncell, 0, 0, 0, 1);
         refine_residual();
-        fetch_states();
-        double prev = h_kst[0].err;
+        // The first pass's inner solve is enqueued before the residual is
+        // read back (one host round trip fewer per solve): when the residual
+        // already meets the tolerance, the finisher has marked the inner
+        // solve done, its kernels return at once and the pass is dropped.
+        bool first = true;
+        double prev = 0;
         refine_fp32_it = 0;
         refine_fp64_it = 0;
         refine_passes = 0;
         bool fallback = false;
         long long used = 0;
         size_t pass = 0;
-        while (!h_kst[0].done) {
+        while (first || !h_kst[0].done) {
             if (last_inner.size() <= pass) last_inner.push_back(0);
             // multigrid-CG: scaled right-hand side, e = 0, first direction
             // (here, not with the residual, so that a rejected pass can
             // still take its correction back)
             if (mg_on) launch_mg_begin(L, mgd, mgb, coef.max_diag, Partials<1>{partial, ticket}, d_kst + 1);
             last_inner[pass] = run_batches(1, last_inner[pass], cap);
+            if (first) {
+                first = false;
+                prev = h_kst[0].err;
+                if (h_kst[0].done) break;  // met before any inner iteration
+            }
             refine_fp32_it += h_kst[1].it;
             refine_passes = (long long)pass + 1;
             if (h_kst[1].breakdown) {  // the correction is discarded, p unchanged

@@ -278,6 +278,26 @@ struct ZlineArgs {
     MgLevel C;
 };
 
+// Position (i, h) of items t0, t0 + nw, t0 + 2 nw, ... of a row-major
+// enumeration with nh items per i, advanced without a division per step.
+struct Stepper {
+    unsigned i, h, di, dh, nh;
+    __device__ __forceinline__ Stepper(unsigned t0, unsigned nw, unsigned nh_) : nh(nh_) {
+        i = t0 / nh;
+        h = t0 - i * nh;
+        di = nw / nh;
+        dh = nw - di * nh;
+    }
+    __device__ __forceinline__ void next() {
+        i += di;
+        h += dh;
+        if (h >= nh) {
+            h -= nh;
+            i++;
+        }
+    }
+};
+
 // The operands of one column's right-hand side in the VEC layout: f and the
 // four x/y neighbours' x of this lane's R rows.
 template <int R>
@@ -676,6 +696,158 @@ k_mg_spmv(MgLevel L, const float *p, float *q, Partials<1> part, KrylovState *st
     }
 }
 
+// The operands of one row of the VEC SpMV: p at the lane's R rows and at
+// its four x/y neighbours, and the values below the lane's first row and
+// above its last row from the guide cells (lanes 0 and 31 only; the other
+// lanes take them from their neighbours by shuffles).
+template <int R>
+struct SpmvLoads {
+    float c[R], e[R], w[R], n[R], s[R];
+    float below, above;
+};
+
+template <int R>
+__device__ __forceinline__ void spmv_load(const MgLevel &L, const float *p, int i, int j,
+                                          int lane, SpmvLoads<R> &v) {
+    const int sx = (int)L.g.sx, sy = (int)L.g.sy;
+    const int c0 = (int)L.at(i, j, 0), cl = c0 + R * lane;  // stored grids have < 2^31 cells
+    load_seg<R>(p + cl, v.c);
+    load_seg<R>(p + (cl + sx), v.e);
+    load_seg<R>(p + (cl - sx), v.w);
+    load_seg<R>(p + (cl + sy), v.n);
+    load_seg<R>(p + (cl - sy), v.s);
+    v.below = lane == 0 ? p[c0 - 1] : 0.f;
+    v.above = lane == 31 ? p[c0 + 32 * R] : 0.f;
+}
+
+// (K p) at the lane's R rows of row (i, j) from the row's operands: the z
+// neighbours across lanes by shuffles (every lane of the warp calls this)
+template <int R>
+__device__ __forceinline__ void row_apply(const MgLevel &L, const SpmvLoads<R> &v, int i, int j,
+                                          int lane, const float (&w2)[R], const float (&zb)[R],
+                                          const float (&zt)[R], float (&out)[R]) {
+    const unsigned full = 0xffffffffu;
+    const float w0 = L.w[0][i], w1 = L.w[1][j];
+    const float xe = L.cf[0][i + 1], xw = L.cf[0][i], yn = L.cf[1][j + 1], ys = L.cf[1][j];
+    const float up = __shfl_down_sync(full, v.c[0], 1);
+    const float dn = __shfl_up_sync(full, v.c[R - 1], 1);
+    const float az = w0 * w1;
+    const float sxy = w1 * (xe + xw) + w0 * (yn + ys);
+#pragma unroll
+    for (int s = 0; s < R; s++) {
+        const float bl = s > 0 ? v.c[s > 0 ? s - 1 : 0] : (lane == 0 ? v.below : dn);
+        const float ab = s < R - 1 ? v.c[s < R - 1 ? s + 1 : 0] : (lane == 31 ? v.above : up);
+        const float diag = w2[s] * sxy + az * (zt[s] + zb[s]);
+        const float nb = w2[s] * (w1 * (xe * v.e[s] + xw * v.w[s]) + w0 * (yn * v.n[s] + ys * v.s[s])) +
+                         az * (zt[s] * ab + zb[s] * bl);
+        out[s] = diag * v.c[s] - nb;
+    }
+}
+
+// the lane's z widths and face conductances: w2, zb (below), zt (above)
+template <int R>
+__device__ __forceinline__ void lane_z(const MgLevel &L, int lane, float (&w2)[R], float (&zb)[R],
+                                       float (&zt)[R]) {
+    load_seg<R>(L.w[2] + R * lane, w2);
+    load_seg<R>(L.cf[2] + R * lane, zb);
+#pragma unroll
+    for (int s = 0; s < R - 1; s++) zt[s] = zb[s + 1];
+    zt[R - 1] = L.cf[2][R * lane + R];
+}
+
+// q = K p and alpha = rho / <p, q> on rows of exactly 32 R cells (the
+// smoother's VEC layout and conditions): one warp per (i, j) row, lane l
+// owning rows k = R l + s, every access a vector access; the z conductances
+// and widths of the lane's rows stay in registers for all the rows the warp
+// visits, and the next row's operands are loaded before this row is
+// computed.  Same operator as MgRow::apply.
+template <int R>
+__global__ void __launch_bounds__(MG_THREADS, R <= 4 ? 3 : 1)
+k_mg_spmv_vec(MgLevel L, const float *p, float *q, Partials<1> part, KrylovState *st) {
+    if (st->done) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned nj = (unsigned)L.n[1], rows = (unsigned)L.n[0] * nj;
+    const unsigned nw = gridDim.x * (blockDim.x >> 5);
+    float w2[R], zb[R], zt[R];
+    lane_z<R>(L, lane, w2, zb, zt);
+    double acc = 0;
+    unsigned row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    Stepper pos(row, nw, nj);
+    SpmvLoads<R> cur, nxt;
+    if (row < rows) spmv_load<R>(L, p, (int)pos.i, (int)pos.h, lane, cur);
+    while (row < rows) {
+        const unsigned row2 = row + nw;
+        const int i = (int)pos.i, j = (int)pos.h;
+        pos.next();
+        if (row2 < rows) spmv_load<R>(L, p, (int)pos.i, (int)pos.h, lane, nxt);
+        float out[R];
+        row_apply<R>(L, cur, i, j, lane, w2, zb, zt, out);
+#pragma unroll
+        for (int s = 0; s < R; s++) acc += (double)cur.c[s] * (double)out[s];
+        store_seg<R>(q + ((int)L.at(i, j, 0) + R * lane), out);
+        row = row2;
+        cur = nxt;
+    }
+    double v[1] = {acc};
+    if (grid_reduce<1>(v, 0u, part) && threadIdx.x == 0) {
+        if (!(v[0] > 0.0) || !isfinite(v[0])) breakdown(st);
+        else st->alpha = st->rho / v[0];
+    }
+}
+
+// The restriction (as k_mg_restrict) from a level of rows of exactly 32 R
+// cells to a coarser one that merges cells along x and/or y only (same z
+// cells, the same vector-row layout on both): one warp per coarse row, the
+// residuals f - K x of its kept children (one or two rows: the colour
+// smoothed last is left out) in the SpMV's row form, their operands loaded
+// together.
+template <int R>
+__global__ void __launch_bounds__(MG_THREADS, R <= 2 ? 3 : R <= 4 ? 2 : 1)
+k_mg_restrict_vec(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, int skip,
+                  const KrylovState *st) {
+    if (st->done) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned nJ = (unsigned)C.n[1], rows = (unsigned)C.n[0] * nJ;
+    const unsigned nw = gridDim.x * (blockDim.x >> 5);
+    float w2[R], zb[R], zt[R];
+    lane_z<R>(F, lane, w2, zb, zt);
+    unsigned row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    Stepper pos(row, nw, nJ);
+    for (; row < rows; row += nw, pos.next()) {
+        const int I = (int)pos.i, J = (int)pos.h;
+        int ci[2] = {0, 0}, cj[2] = {0, 0}, kept = 0;
+        for (int a = 0; a < C.fac[0]; a++)
+            for (int b = 0; b < C.fac[1]; b++) {
+                const int i = I * C.fac[0] + a, j = J * C.fac[1] + b;
+                if (((i + j) & 1) != skip && kept < 2) {
+                    ci[kept] = i;
+                    cj[kept] = j;
+                    kept++;
+                }
+            }
+        SpmvLoads<R> v[2];
+        float fv[2][R];
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+            if (c < kept) {
+                spmv_load<R>(F, x, ci[c], cj[c], lane, v[c]);
+                load_seg<R>(f + F.at(ci[c], cj[c], 0) + R * lane, fv[c]);
+            }
+        float sum[R];
+#pragma unroll
+        for (int s = 0; s < R; s++) sum[s] = 0.f;
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+            if (c < kept) {
+                float kx[R];
+                row_apply<R>(F, v[c], ci[c], cj[c], lane, w2, zb, zt, kx);
+#pragma unroll
+                for (int s = 0; s < R; s++) sum[s] += fv[c][s] - kx[s];
+            }
+        store_seg<R>(fc + C.at(I, J, 0) + R * lane, sum);
+    }
+}
+
 // e += alpha p, r -= alpha q; err = RMS of r / (-max_diag vol); stop test
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_update(MgLevel L, float *e, float *r, const float *p, const float *q, float md,
@@ -737,6 +909,18 @@ k_mg_pupdate(MgLevel L, const float *z, float *p, const KrylovState *st) {
         [&](long long c0, int k, float2 v) { p[c0 + k] = v.x + b * v.y; });
 }
 
+// R of the VEC SpMV for this level and these vectors (rows of exactly 32 R
+// cells, R = 1, 2, 4, 8; every row start and stride a multiple of 8
+// elements; 16-byte aligned vectors and z arrays), else 0
+int spmv_vec_r(const MgLevel &v, const float *p, const float *q) {
+    auto al = [](const void *x) { return ((uintptr_t)x & 15) == 0; };
+    const int nk = v.n[2], R = nk / 32;
+    const bool ok = nk % 32 == 0 && (R == 1 || R == 2 || R == 4 || R == 8) &&
+                    v.at(0, 0, 0) % 8 == 0 && v.g.sx % 8 == 0 && v.g.sy % 8 == 0 && al(p) &&
+                    al(q) && al(v.w[2]) && al(v.cf[2]);
+    return ok ? R : 0;
+}
+
 int blocks_for(long long n, int cap) {
     long long b = (n + MG_THREADS - 1) / MG_THREADS;
     if (b < 1) b = 1;
@@ -771,9 +955,21 @@ struct DeviceCycle {
         last_color[l] = color;
     }
     void restrict(int l) {
+        const MgLevel &F = M.L[l], &C = M.L[l + 1];
+        const int nb = blocks_for(C.cells(), L.blocks);
+        const int r = C.fac[2] == 1 && C.n[2] == F.n[2] && spmv_vec_r(C, M.f[l + 1], M.f[l + 1])
+                          ? spmv_vec_r(F, M.x[l], M.f[l])
+                          : 0;
         L.pre(KK_MG_TRANSFER);
-        k_mg_restrict<<<blocks_for(M.L[l + 1].cells(), L.blocks), MG_THREADS, 0, L.s>>>(
-            M.L[l], M.L[l + 1], M.x[l], M.f[l], M.f[l + 1], last_color[l], st);
+        switch (r) {
+        case 1: k_mg_restrict_vec<1><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        case 2: k_mg_restrict_vec<2><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        case 4: k_mg_restrict_vec<4><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        case 8: k_mg_restrict_vec<8><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        default:
+            k_mg_restrict<<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st);
+            break;
+        }
         L.post(KK_MG_TRANSFER);
         // R x, f of half the children; W the coarse f
         L.bytes(KK_MG_TRANSFER, 4.0 * ((double)M.L[l].cells() + 0.5 * (double)M.L[l].cells() +
@@ -828,7 +1024,13 @@ void launch_mg_iteration(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B,
     const MgLevel &v = M.L[0];
     const double n = (double)v.cells();
     L.pre(KK_MG_PCG);
-    k_mg_spmv<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st);
+    switch (spmv_vec_r(v, B.p, B.q)) {
+    case 1: k_mg_spmv_vec<1><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
+    case 2: k_mg_spmv_vec<2><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
+    case 4: k_mg_spmv_vec<4><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
+    case 8: k_mg_spmv_vec<8><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
+    default: k_mg_spmv<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
+    }
     L.post(KK_MG_PCG);
     L.bytes(KK_MG_PCG, 8.0 * n);  // R p; W q
     L.pre(KK_MG_PCG);

@@ -264,3 +264,53 @@ def test_mixed_multi_tile_grid(make_case):
         worst["p"] = max(worst["p"], rel(s.field("p"), o.field("p")))
     print("multi-tile mixed vs oracle:", worst)
     assert worst["U"] <= 5e-6 and worst["p"] <= 2e-2, worst
+
+
+# (case, cells, overrides): z columns of exactly 32 R cells, R = 2 and 4.
+# The second grid is 20 tall so that its wall cells (3.5e-3) keep the
+# explicit scheme stable at dt = 2.5e-4 (at height 5 the 8.8e-4 wall cells
+# under the uniform inflow's wall shear put the Smagorinsky diffusion number
+# near 2, and the reference's scheme diverges).
+VEC_ROWS = [("tiny-loglaw", (48, 24, 64), {"dt": 5e-4}),
+            ("tiny-bicg", (32, 16, 128), {"dt": 2.5e-4, "lengths": (2.0, 1.0, 20.0)})]
+
+
+@pytest.mark.parametrize("name,n,over", VEC_ROWS, ids=["R2", "R4"])
+def test_multigrid_vector_rows(make_case, monkeypatch, capfd, name, n, over):
+    """The multigrid-CG inner solve's level-0 kernels on z columns of exactly
+    32 R cells, where the SpMV and the smoother take the vector-row layout
+    (one warp per row, lane l owning rows R l .. R l + R - 1): every solve
+    meets the case's tolerance by FP32 passes alone, in few multigrid-CG
+    iterations (an operator that is not K would stall conjugate gradients
+    and hand the solve to the FP64 fallback), and U stays within the
+    envelope of the FP64 form."""
+    pkg = package()
+    spec, mesh, d, U0, prof = make_case(name, n=n, **over)
+    monkeypatch.setenv("DALM_TRACE_POISSON", "1")
+    s = pkg.Solver(d, precision=pkg.MIXED)
+    monkeypatch.delenv("DALM_TRACE_POISSON")
+    f = pkg.Solver(d, precision=pkg.FP64)
+    for x in (s, f):
+        if prof is not None:
+            x.set_inflow_profile(prof)
+        x.set_state(U0)
+    worst = 0.0
+    for k in range(6):
+        s.step(1)
+        f.step(1)
+        if k >= 1:
+            assert s.stats()["err"] <= spec.tol, (k, s.stats())
+        U, Uf = s.field("U"), f.field("U")
+        worst = max(worst, max(rel(U[..., m], Uf[..., m]) for m in range(3)))
+    solves = []
+    for line in capfd.readouterr().err.splitlines():
+        if "poisson it" in line and "FP32" in line:
+            t = line.split("(FP32 ")[1]
+            fp32, rest = t.split(" in ")
+            passes, fp64 = rest.split(" passes, FP64 ")
+            solves.append((int(fp32), int(passes), int(fp64.rstrip(")"))))
+    print(n, "FP32 its, passes, FP64 its per solve:", solves, "U vs FP64:", worst)
+    assert len(solves) >= 5
+    for fp32, passes, fp64 in solves:
+        assert fp64 == 0 and passes <= 3 and fp32 <= 8 * max(passes, 1), solves
+    assert worst <= MIXED_ENVELOPE["U"], worst
