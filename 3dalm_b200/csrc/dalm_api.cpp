@@ -838,7 +838,9 @@ struct dalm_handle {
     // FP64 residual of the pressure, its norm and the stop test; the next
     // inner solve's right-hand side in FP32
     void refine_residual() {
-        launch_refine_residual(L, g, coef, pcfg, Pp, B, pbf, Partials<2>{partial, ticket}, d_kst,
+        PoissonBufsT<float> in = pbf;
+        if (mg_on) in.r0 = in.q = nullptr;  // multigrid-CG reads the residual alone
+        launch_refine_residual(L, g, coef, pcfg, Pp, B, in, Partials<2>{partial, ticket}, d_kst,
                                d_kst + 1);
     }
     void solve_mixed() {
@@ -2128,7 +2130,9 @@ int dalm_get_kernel_timing(dalm_handle *h, int index, const char **name, int64_t
         case KK_BICG_XR: s = 8 * n; break;
         case KK_BICG_PF: s = 7 * n; break;
         case KK_BICG_SF: s = 5 * n; break;
-        case KK_REFINE_RESIDUAL: s = 3.5 * n; break;  // R x, b (FP64); W r, r0, q (FP32)
+        case KK_REFINE_RESIDUAL:  // R x, b (FP64); W r (FP32) [, r0, q for BiCGStab inner solves]
+            s = (h->mg_on ? 2.5 : 3.5) * n;
+            break;
         case KK_REFINE_UPDATE: s = 2.5 * n; break;    // R x, e; W x
         // FP32 vectors: half the scalars' bytes
         case KK_SOR_SWEEP32: s = 2 * n / 2.0; break;

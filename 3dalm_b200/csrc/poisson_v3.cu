@@ -236,7 +236,7 @@ enum StencilKind {
     SK_Q = 3,         // q = A pp, sum r0*q                       src/eq.h:369-371
     SK_T = 4,         // t = A ss, sum t*s, sum t*t               src/eq.h:381-383
     SK_SOR = 5,       // red-black update in place                src/eq.h:145-181
-    SK_REFINE = 6     // FP64 r = b - A x; FP32 inner r = r0 = r, q = 0; sums r*r
+    SK_REFINE = 6     // FP64 r = b - A x; FP32 inner r [= r0, q = 0]; sums r*r
 };
 
 struct StencilArgs {
@@ -343,8 +343,8 @@ k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
             const double r = (double)pw - (double)ax;
             const float r32 = (float)r;
             ((float *)A.out)[c] = r32;
-            ((float *)A.out2)[c] = r32;
-            ((float *)A.out3)[c] = 0.f;
+            if (A.out2) ((float *)A.out2)[c] = r32;  // BiCGStab inner solves only
+            if (A.out3) ((float *)A.out3)[c] = 0.f;
             acc0 += r * r;
             acc1 += (double)r32 * (double)r32;
         }

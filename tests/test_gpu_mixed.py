@@ -124,6 +124,9 @@ def test_multigrid_inner_solves(make_case):
     assert kt["mg_pcg"]["launches"] > 0
     assert kt["bicg_xr32"]["launches"] == 0 and kt["jacobi_sweep32"]["launches"] == 0
     assert sum(its_m) * 5 <= sum(its_f)
+    # the FP64 residual writes only the FP32 residual for multigrid-CG
+    cells = int(np.prod([n - 2 * s.gc for n in s.size]))
+    assert kt["refine_residual"]["bytes_per_launch"] == 20.0 * cells
 
 
 def is_fp32(v):
