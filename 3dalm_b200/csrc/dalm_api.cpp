@@ -918,7 +918,6 @@ struct dalm_handle {
             jcur = 1 - jcur;
             launch_velocity_bc(L, P, u_cur(), c(u_old()));
         }
-        DALM_CUDA(cudaMemcpyAsync(h_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToHost, stream));
     }
 
     // Blade-point positions on the host (same formulas as the device) to
@@ -1113,10 +1112,6 @@ struct dalm_handle {
             launch_alm_project(L, P, alm, unite(fbox, cur), f3());
             fbox = cur;
         }
-        DALM_CUDA(cudaMemcpyAsync(h_wt_out, alm.wt_torque, sizeof(double) * alm.wt_count,
-                                  cudaMemcpyDeviceToHost, stream));
-        DALM_CUDA(cudaMemcpyAsync(h_wt_out + alm.wt_count, alm.wt_thrust, sizeof(double) * alm.wt_count,
-                                  cudaMemcpyDeviceToHost, stream));
     }
     void stage_diag() {
         StageTimer t(this, DALM_STAGE_DIAG);
@@ -1680,6 +1675,7 @@ struct dalm_handle {
             if (n >= last0) record(n - last0, true);
             step_once();
             if (n >= t0) {
+                fetch_step_outputs();
                 DALM_CUDA(cudaStreamSynchronize(stream));
                 for (int w = 0; w < T; w++) J += h_wt_out[w] * std::fabs(h_wt[w].rot_speed);
             }
@@ -1693,6 +1689,7 @@ struct dalm_handle {
         KrylovState *fin_kst = S.get<KrylovState>(2);
         DALM_CUDA(cudaMemcpyAsync(fin_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToDevice, stream));
         DALM_CUDA(cudaMemcpyAsync(fin_kst, d_kst, 2 * sizeof(KrylovState), cudaMemcpyDeviceToDevice, stream));
+        fetch_step_outputs();
         DALM_CUDA(cudaStreamSynchronize(stream));
         KrylovState fin_hkst[2] = {h_kst[0], h_kst[1]};
         DiagState fin_hdiag = *h_diag;
@@ -1761,7 +1758,20 @@ struct dalm_handle {
         if (J_out) *J_out = J;
     }
 
+    // The last step's diagnostics and turbine loads into their pinned host
+    // copies, enqueued where a reader is about to synchronise rather than
+    // every step (each small copy costs the stream a few microseconds).
+    void fetch_step_outputs() {
+        DALM_CUDA(cudaMemcpyAsync(h_diag, d_diag, sizeof(DiagState), cudaMemcpyDeviceToHost, stream));
+        if (alm.ap_count > 0) {
+            DALM_CUDA(cudaMemcpyAsync(h_wt_out, alm.wt_torque, sizeof(double) * alm.wt_count,
+                                      cudaMemcpyDeviceToHost, stream));
+            DALM_CUDA(cudaMemcpyAsync(h_wt_out + alm.wt_count, alm.wt_thrust,
+                                      sizeof(double) * alm.wt_count, cudaMemcpyDeviceToHost, stream));
+        }
+    }
     void sync_stats() {
+        fetch_step_outputs();
         DALM_CUDA(cudaStreamSynchronize(stream));
         if (opt.profile) harvest();
     }
