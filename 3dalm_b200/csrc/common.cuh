@@ -10,6 +10,7 @@
 // 8 (FP64) or 4 (FP32) 32-byte sectors.
 #pragma once
 
+#include <utility>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -287,6 +288,37 @@ struct LaunchCtx {
         DALM_CUDA(cudaGetLastError());
     }
 };
+
+// Programmatic dependent launch: a kernel launched by pdl_launch may be
+// scheduled while the previous kernel in the stream is finishing, so its
+// launch latency overlaps that kernel's tail.  pdl_wait(), the first
+// statement of every such kernel, holds it until the previous kernel has
+// completed and its memory operations are visible (griddepcontrol.wait; a
+// no-op when the kernel was launched without the attribute); it then lets
+// the next kernel be scheduled as soon as every block of this one has
+// started (griddepcontrol.launch_dependents: the waiting blocks of the next
+// kernel never hold back a block of this one, which are all resident by
+// then).
+__device__ __forceinline__ void pdl_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
+}
+
+template <typename... Exp, typename... Act>
+inline void pdl_launch(void (*kernel)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Act &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    DALM_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Act>(args)...));
+}
 
 inline int reduction_blocks(int sm_count) { return sm_count * 8; }
 

@@ -331,6 +331,7 @@ __device__ __forceinline__ void zline_load(const MgLevel &L, const float *x, con
 // arithmetic as k_mg_smooth's VEC path.
 template <int R, bool FAC>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth_pipe(ZlineArgs A, const KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     const MgLevel &L = A.L;
     float *__restrict__ x = A.x;
@@ -498,6 +499,7 @@ __device__ __forceinline__ void zline_solve_column(const ZlineArgs &A, int i, in
 
 template <int R, bool FAC, bool VEC>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(ZlineArgs A, const KrylovState *st) {
+    pdl_wait();
     __shared__ float slab[MG_THREADS / 32][33 * R];
     if (st->done) return;
     const int lane = threadIdx.x & 31;
@@ -532,17 +534,17 @@ template <int R>
 void zline_launch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st, int blocks) {
     const bool vec = zline_vec_ok(a, R);
     if (vec && !a.xc && a.L.ltab)
-        k_mg_smooth_pipe<R, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+        pdl_launch(k_mg_smooth_pipe<R, true>, blocks, MG_THREADS, 0, L.s, a, st);
     else if (vec && !a.xc)
-        k_mg_smooth_pipe<R, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+        pdl_launch(k_mg_smooth_pipe<R, false>, blocks, MG_THREADS, 0, L.s, a, st);
     else if (a.L.ltab && vec)
-        k_mg_smooth<R, true, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+        pdl_launch(k_mg_smooth<R, true, true>, blocks, MG_THREADS, 0, L.s, a, st);
     else if (a.L.ltab)
-        k_mg_smooth<R, true, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+        pdl_launch(k_mg_smooth<R, true, false>, blocks, MG_THREADS, 0, L.s, a, st);
     else if (vec)
-        k_mg_smooth<R, false, true><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+        pdl_launch(k_mg_smooth<R, false, true>, blocks, MG_THREADS, 0, L.s, a, st);
     else
-        k_mg_smooth<R, false, false><<<blocks, MG_THREADS, 0, L.s>>>(a, st);
+        pdl_launch(k_mg_smooth<R, false, false>, blocks, MG_THREADS, 0, L.s, a, st);
 }
 
 void zline_dispatch(const LaunchCtx &L, const ZlineArgs &a, const KrylovState *st) {
@@ -611,6 +613,7 @@ __device__ __forceinline__ void mg_restrict_rows(const MgLevel &F, const MgLevel
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_restrict(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, int skip,
               const KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     mg_restrict_rows(F, C, x, f, fc, skip, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5),
                      gridDim.x * (blockDim.x >> 5));
@@ -633,6 +636,7 @@ __device__ __forceinline__ void mg_coarse_rows(const MgLevel &C, const float *ki
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_coarse(MgLevel C, const float *kinv, int n, const float *f, float *x,
             const KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     mg_coarse_rows(C, kinv, n, f, x, blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5),
                    gridDim.x * (blockDim.x >> 5));
@@ -641,6 +645,7 @@ k_mg_coarse(MgLevel C, const float *kinv, int n, const float *f, float *x,
 // f = -max_diag vol r (in place), e = 0
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_rhs(MgLevel L, float *r, float *e, float md, const KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     level_loop<4>(
         L, [&](int i, int j) { return row_base(L, i, j); },
@@ -660,6 +665,7 @@ __device__ __forceinline__ void breakdown(KrylovState *st) {
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_first(MgLevel L, const float *r, const float *z, float *p, Partials<1> part,
            KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     double acc = 0;
     level_loop<4>(
@@ -680,6 +686,7 @@ k_mg_first(MgLevel L, const float *r, const float *z, float *p, Partials<1> part
 // q = K p; alpha = rho / <p, q>
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_spmv(MgLevel L, const float *p, float *q, Partials<1> part, KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     double acc = 0;
     level_loop<4>(
@@ -764,6 +771,7 @@ __device__ __forceinline__ void lane_z(const MgLevel &L, int lane, float (&w2)[R
 template <int R>
 __global__ void __launch_bounds__(MG_THREADS, R <= 4 ? 3 : 1)
 k_mg_spmv_vec(MgLevel L, const float *p, float *q, Partials<1> part, KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     const int lane = threadIdx.x & 31;
     const unsigned nj = (unsigned)L.n[1], rows = (unsigned)L.n[0] * nj;
@@ -805,6 +813,7 @@ template <int R>
 __global__ void __launch_bounds__(MG_THREADS, R <= 2 ? 3 : R <= 4 ? 2 : 1)
 k_mg_restrict_vec(MgLevel F, MgLevel C, const float *x, const float *f, float *fc, int skip,
                   const KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     const int lane = threadIdx.x & 31;
     const unsigned nJ = (unsigned)C.n[1], rows = (unsigned)C.n[0] * nJ;
@@ -852,6 +861,7 @@ k_mg_restrict_vec(MgLevel F, MgLevel C, const float *x, const float *f, float *f
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_update(MgLevel L, float *e, float *r, const float *p, const float *q, float md,
             Partials<1> part, KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     const float a = (float)st->alpha;
     double acc = 0;
@@ -881,6 +891,7 @@ k_mg_update(MgLevel L, float *e, float *r, const float *p, const float *q, float
 // beta = <r, z> / rho, rho = <r, z>
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_rz(MgLevel L, const float *r, const float *z, Partials<1> part, KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     double acc = 0;
     level_loop<4>(
@@ -901,6 +912,7 @@ k_mg_rz(MgLevel L, const float *r, const float *z, Partials<1> part, KrylovState
 // p = z + beta p
 __global__ void __launch_bounds__(MG_THREADS)
 k_mg_pupdate(MgLevel L, const float *z, float *p, const KrylovState *st) {
+    pdl_wait();
     if (st->done) return;
     const float b = (float)st->beta;
     level_loop<4>(
@@ -962,12 +974,12 @@ struct DeviceCycle {
                           : 0;
         L.pre(KK_MG_TRANSFER);
         switch (r) {
-        case 1: k_mg_restrict_vec<1><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
-        case 2: k_mg_restrict_vec<2><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
-        case 4: k_mg_restrict_vec<4><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
-        case 8: k_mg_restrict_vec<8><<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        case 1: pdl_launch(k_mg_restrict_vec<1>, nb, MG_THREADS, 0, L.s, F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        case 2: pdl_launch(k_mg_restrict_vec<2>, nb, MG_THREADS, 0, L.s, F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        case 4: pdl_launch(k_mg_restrict_vec<4>, nb, MG_THREADS, 0, L.s, F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
+        case 8: pdl_launch(k_mg_restrict_vec<8>, nb, MG_THREADS, 0, L.s, F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st); break;
         default:
-            k_mg_restrict<<<nb, MG_THREADS, 0, L.s>>>(F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st);
+            pdl_launch(k_mg_restrict, nb, MG_THREADS, 0, L.s, F, C, M.x[l], M.f[l], M.f[l + 1], last_color[l], st);
             break;
         }
         L.post(KK_MG_TRANSFER);
@@ -978,8 +990,8 @@ struct DeviceCycle {
     void coarse() {
         const int l = M.levels - 1;
         L.pre(KK_MG_COARSE);
-        k_mg_coarse<<<blocks_for((long long)M.ncoarse * 32, L.blocks), MG_THREADS, 0, L.s>>>(
-            M.L[l], M.kinv, M.ncoarse, M.f[l], M.x[l], st);
+        pdl_launch(k_mg_coarse, blocks_for((long long)M.ncoarse * 32, L.blocks), MG_THREADS, 0, L.s,
+                   M.L[l], M.kinv, M.ncoarse, M.f[l], M.x[l], st);
         L.post(KK_MG_COARSE);
         L.bytes(KK_MG_COARSE, 4.0 * ((double)M.ncoarse * M.ncoarse + 2.0 * M.ncoarse));
     }
@@ -1006,7 +1018,7 @@ void launch_mg_begin(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B, dou
     const int nb = blocks_for(v.cells(), L.blocks);
     const double n = (double)v.cells();
     L.pre(KK_MG_PCG);
-    k_mg_rhs<<<nb, MG_THREADS, 0, L.s>>>(v, B.r, B.e, (float)max_diag, st);
+    pdl_launch(k_mg_rhs, nb, MG_THREADS, 0, L.s, v, B.r, B.e, (float)max_diag, st);
     L.post(KK_MG_PCG);
     L.bytes(KK_MG_PCG, 12.0 * n);  // R r; W r, e
     MgDev m = M;
@@ -1014,7 +1026,7 @@ void launch_mg_begin(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B, dou
     m.x[0] = B.z;
     launch_mg_vcycle(L, m, st);
     L.pre(KK_MG_PCG);
-    k_mg_first<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.r, B.z, B.p, part, st);
+    pdl_launch(k_mg_first, L.blocks, MG_THREADS, 0, L.s, v, B.r, B.z, B.p, part, st);
     L.post(KK_MG_PCG);
     L.bytes(KK_MG_PCG, 12.0 * n);  // R r, z; W p
 }
@@ -1025,16 +1037,16 @@ void launch_mg_iteration(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B,
     const double n = (double)v.cells();
     L.pre(KK_MG_PCG);
     switch (spmv_vec_r(v, B.p, B.q)) {
-    case 1: k_mg_spmv_vec<1><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
-    case 2: k_mg_spmv_vec<2><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
-    case 4: k_mg_spmv_vec<4><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
-    case 8: k_mg_spmv_vec<8><<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
-    default: k_mg_spmv<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.p, B.q, part, st); break;
+    case 1: pdl_launch(k_mg_spmv_vec<1>, L.blocks, MG_THREADS, 0, L.s, v, B.p, B.q, part, st); break;
+    case 2: pdl_launch(k_mg_spmv_vec<2>, L.blocks, MG_THREADS, 0, L.s, v, B.p, B.q, part, st); break;
+    case 4: pdl_launch(k_mg_spmv_vec<4>, L.blocks, MG_THREADS, 0, L.s, v, B.p, B.q, part, st); break;
+    case 8: pdl_launch(k_mg_spmv_vec<8>, L.blocks, MG_THREADS, 0, L.s, v, B.p, B.q, part, st); break;
+    default: pdl_launch(k_mg_spmv, L.blocks, MG_THREADS, 0, L.s, v, B.p, B.q, part, st); break;
     }
     L.post(KK_MG_PCG);
     L.bytes(KK_MG_PCG, 8.0 * n);  // R p; W q
     L.pre(KK_MG_PCG);
-    k_mg_update<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.e, B.r, B.p, B.q, (float)max_diag, part, st);
+    pdl_launch(k_mg_update, L.blocks, MG_THREADS, 0, L.s, v, B.e, B.r, B.p, B.q, (float)max_diag, part, st);
     L.post(KK_MG_PCG);
     L.bytes(KK_MG_PCG, 24.0 * n);  // R e, p, r, q; W e, r
     MgDev m = M;
@@ -1042,11 +1054,11 @@ void launch_mg_iteration(const LaunchCtx &L, const MgDev &M, const MgPcgBufs &B,
     m.x[0] = B.z;
     launch_mg_vcycle(L, m, st);
     L.pre(KK_MG_PCG);
-    k_mg_rz<<<L.blocks, MG_THREADS, 0, L.s>>>(v, B.r, B.z, part, st);
+    pdl_launch(k_mg_rz, L.blocks, MG_THREADS, 0, L.s, v, B.r, B.z, part, st);
     L.post(KK_MG_PCG);
     L.bytes(KK_MG_PCG, 8.0 * n);  // R r, z
     L.pre(KK_MG_PCG);
-    k_mg_pupdate<<<blocks_for(v.cells(), L.blocks), MG_THREADS, 0, L.s>>>(v, B.z, B.p, st);
+    pdl_launch(k_mg_pupdate, blocks_for(v.cells(), L.blocks), MG_THREADS, 0, L.s, v, B.z, B.p, st);
     L.post(KK_MG_PCG);
     L.bytes(KK_MG_PCG, 12.0 * n);  // R z, p; W p
 }
