@@ -52,25 +52,34 @@ __device__ __forceinline__ void minmod_pair(float a, float b, float bb, float &g
 // Upwind flux through the face between cells c and p = c + 1 along one axis
 // from the values at c - 1, c, c + 1, c + 2 and the face's volume flux J
 // (src/cfd.h:37-60: kappa = 1/3 MUSCL with the b = 4 limiter, or the smooth
-// van Albada limiter of DALM_LIMITER_VAN_ALBADA).
+// van Albada limiter of DALM_LIMITER_VAN_ALBADA).  The reference blends the
+// left and right states, 0.5 (J (fr + fl) - |J| (fr - fl)), which is J fl
+// for J > 0 and J fr otherwise; only that upwind state is formed here, so
+// each face takes one limiter evaluation instead of two.  The two states are
+// one reconstruction mirrored: with centre u, forward difference a and
+// backward difference b (fl: u = fc, a = fp - fc, b = fc - fm; fr: u = fp,
+// a = fc - fp, b = fp - fpp) the state is
+//   u + 1/4 [(1 - kappa) L(b, a) + (1 + kappa) L(a, b)]
+// with L(x, y) = minmod(x, bb y) for b = 4 (odd in its arguments) or
+// s x, s = (2ab + eps) / (a^2 + b^2 + eps), for van Albada (even).
 __device__ __forceinline__ float face_flux(float fm, float fc, float fp, float fpp, float J,
                                            int limiter) {
     const float kap = 1.f / 3.f;
     const float bb = (3.f - kap) / (1.f - kap);
-    const float d4 = fpp - fp, d3 = fp - fc, d2 = fc - fm;
-    float fr, fl;  // right and left states at the face
+    const bool pos = J > 0.f;
+    const float u = pos ? fc : fp;
+    const float a = pos ? fp - fc : fc - fp;
+    const float b = pos ? fc - fm : fp - fpp;
+    float st;
     if (limiter == 1) {
-        const float sp = va_switch_f(d4, d3), sc = va_switch_f(d3, d2);
-        fr = fp - (sp * 0.25f) * ((1.f - kap * sp) * d4 + (1.f + kap * sp) * d3);
-        fl = fc + (sc * 0.25f) * ((1.f - kap * sc) * d2 + (1.f + kap * sc) * d3);
+        const float s = va_switch_f(a, b);
+        st = u + (s * 0.25f) * ((1.f - kap * s) * b + (1.f + kap * s) * a);
     } else {
-        float g6, g5, g4, g3;
-        minmod_pair(d4, d3, bb, g6, g5);
-        minmod_pair(d3, d2, bb, g4, g3);
-        fr = fp - 0.25f * ((1.f - kap) * g6 + (1.f + kap) * g5);
-        fl = fc + 0.25f * ((1.f - kap) * g3 + (1.f + kap) * g4);
+        float lab, lba;  // L(a, b), L(b, a)
+        minmod_pair(a, b, bb, lab, lba);
+        st = u + 0.25f * ((1.f - kap) * lba + (1.f + kap) * lab);
     }
-    return 0.5f * (J * (fr + fl) - fabsf(J) * (fr - fl));
+    return J * st;
 }
 
 constexpr int HR = TJ + 4;  // tile rows: j - 2 .. j + 9
