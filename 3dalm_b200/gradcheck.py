@@ -12,11 +12,22 @@ from fresh forward runs, and prints one JSON object with both, their
 relative differences and the run times.  The pressure solves run to --tol
 (RMS residual) so that the forward's solver tolerance enters the finite
 differences as little as possible.
+
+Under torchrun (WORLD_SIZE > 1) the check runs as replicas, one per GPU:
+the forward runs of the finite differences are independent, so rank r
+takes every WORLD_SIZE-th of them on device LOCAL_RANK, rank 0 also runs
+the adjoint, and the objective values meet on rank 0 through one host-side
+gather (gloo); nothing crosses between GPUs.
+
+    python -m torch.distributed.run --nproc-per-node 8 --master-addr 127.0.0.1 \
+        -m 3dalm_b200.gradcheck c5 --tol 1e-13 --h 1e-4
 """
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
+import os
 import shutil
 import tempfile
 import time
@@ -27,6 +38,56 @@ from . import VAN_ALBADA, Solver
 from . import casegen
 
 KINDS = {"yaw": 0, "pitch": 1, "omega": 2}
+
+
+def fd_jobs(nturb, kinds, hs):
+    """The forward runs of the central differences: (h, turbine, kind, sign)
+    for every step size, turbine and parameter kind, + before -."""
+    return [(h, w, q, sgn) for h in hs for w in range(nturb) for q in kinds for sgn in (1, -1)]
+
+
+def run_jobs(jobs, objective, base, rank=0, world=1):
+    """Objective values of this rank's share of the jobs (every world-th,
+    from rank): {job index: J}.  base: (yaw, pitch, omega) arrays."""
+    out = {}
+    for i in range(rank, len(jobs), world):
+        h, w, q, sgn = jobs[i]
+        p = [np.array(v, dtype=float) for v in base]
+        p[q][w] += sgn * h
+        out[i] = objective(p)
+    return out
+
+
+def assemble(jobs, values, nturb):
+    """{h: (nturb x 3) central differences} from all jobs' values (NaN where
+    a kind was not differenced)."""
+    fd = {}
+    for i, (h, w, q, sgn) in enumerate(jobs):
+        a = fd.setdefault(h, np.full((nturb, 3), np.nan))
+        if sgn == 1:
+            a[w, q] = (values[i] - values[i + 1]) / (2 * h)
+    return fd
+
+
+def replicas():
+    """(rank, world, local_rank, gather) under torchrun, else (0, 1, 0,
+    identity).  gather(dict) merges every rank's dict (host-side, gloo)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return 0, 1, 0, lambda d: d
+    import torch.distributed as dist
+    if not dist.is_initialized():
+        dist.init_process_group("gloo", timeout=datetime.timedelta(hours=4))
+
+    def gather(d):
+        parts = [None] * dist.get_world_size()
+        dist.all_gather_object(parts, d)
+        merged = {}
+        for part in parts:
+            merged.update(part)
+        return merged
+
+    return dist.get_rank(), dist.get_world_size(), int(os.environ.get("LOCAL_RANK", "0")), gather
 
 
 def main(argv=None):
@@ -45,15 +106,17 @@ def main(argv=None):
     ap.add_argument("--case-dir", default=None)
     ap.add_argument("--no-fd", action="store_true", help="adjoint and one forward run only")
     a = ap.parse_args(argv)
+    rank, world, device, gather = replicas()
 
     spec = casegen.config(a.config, steps=a.steps)
-    d = a.case_dir or tempfile.mkdtemp(prefix="dalm_gradcheck_")
+    d = (os.path.join(a.case_dir, f"rank{rank}") if a.case_dir and world > 1 else a.case_dir) \
+        or tempfile.mkdtemp(prefix="dalm_gradcheck_")
     mesh = casegen.write_case(spec, d)
     U0 = casegen.initial_velocity(spec, mesh)
     prof = casegen.inflow_profile(spec, mesh)
 
     def make(params=None):
-        s = Solver(d, limiter=VAN_ALBADA, time_average=False)
+        s = Solver(d, limiter=VAN_ALBADA, time_average=False, device=device)
         if prof is not None:
             s.set_inflow_profile(prof)
         s.set_poisson(a.max_it, a.tol)
@@ -75,14 +138,17 @@ def main(argv=None):
 
     s = make()
     base = s.turbine_params()
-    t = time.perf_counter()
-    J, g = s.power_gradient(a.t0, a.steps, a.ckpt)
-    t_adj = time.perf_counter() - t
-    stats = s.adjoint_stats()
+    nturb = len(base[0])
+    J, g, t_adj, stats = np.nan, np.full((nturb, 3), np.nan), 0.0, {}
+    if rank == 0:
+        t = time.perf_counter()
+        J, g = s.power_gradient(a.t0, a.steps, a.ckpt)
+        t_adj = time.perf_counter() - t
+        stats = s.adjoint_stats()
     s.close()
     t = time.perf_counter()
-    J_fwd = objective(base)
-    t_fwd = time.perf_counter() - t
+    fwd = gather({"J": objective(base), "s": time.perf_counter() - t} if rank == world - 1 else {})
+    J_fwd, t_fwd = fwd["J"], fwd["s"]
     out = {
         "config": a.config, "cells": list(spec.n), "turbines": len(base[0]),
         "steps": a.steps, "window": [a.t0, a.steps], "ckpt_every": a.ckpt,
@@ -91,20 +157,9 @@ def main(argv=None):
                    "omega": base[2].tolist()},
         "J": J, "J_forward": J_fwd, "grad": g.tolist(),
         "adjoint_s": t_adj, "forward_s": t_fwd, "adjoint_over_forward": t_adj / t_fwd,
-        "adjoint_stats": stats,
+        "adjoint_stats": stats, "replicas": world,
     }
     kinds = [KINDS[a.only]] if a.only else [0, 1, 2]
-
-    def central(h):
-        fd = np.full_like(g, np.nan)
-        for w in range(g.shape[0]):
-            for q in kinds:
-                pp = [v.copy() for v in base]
-                pm = [v.copy() for v in base]
-                pp[q][w] += h
-                pm[q][w] -= h
-                fd[w, q] = (objective(pp) - objective(pm)) / (2 * h)
-        return fd
 
     def report(fd):
         m = ~np.isnan(fd)
@@ -115,12 +170,18 @@ def main(argv=None):
                 "norm_rel_err": float(np.linalg.norm((g - fd)[m]) / np.linalg.norm(fd[m]))}
 
     if not a.no_fd:
+        hs = [a.h] + list(a.h_list or [])
+        jobs = fd_jobs(nturb, kinds, hs)
         t = time.perf_counter()
-        out.update(report(central(a.h)))
+        values = gather(run_jobs(jobs, objective, base, rank, world))
+        fd = assemble(jobs, values, nturb)
         out["fd_s"] = time.perf_counter() - t
-        for h in a.h_list or []:
-            out.setdefault("fd_h", {})[repr(h)] = report(central(h))
-    print(json.dumps(out))
+        if rank == 0:  # the adjoint gradient lives on rank 0
+            out.update(report(fd[a.h]))
+            for h in hs[1:]:
+                out.setdefault("fd_h", {})[repr(h)] = report(fd[h])
+    if rank == 0:
+        print(json.dumps(out))
     if not a.case_dir:
         shutil.rmtree(d, ignore_errors=True)
 
