@@ -261,6 +261,8 @@ enum KernelKind {
     KK_ADJ_BC, KK_ADJ_PROJECT, KK_ADJ_FACES, KK_ADJ_NUT, KK_ADJ_PREDICT, KK_ADJ_ALM,
     // multigrid-preconditioned CG (inner solves of DALM_MIXED)
     KK_MG_SMOOTH, KK_MG_TRANSFER, KK_MG_COARSE, KK_MG_PCG,
+    // two FP64 Jacobi sweeps in one pass (the preconditioner's last two)
+    KK_JACOBI_SWEEP2,
     KK_COUNT
 };
 

@@ -63,7 +63,8 @@ const char *kKindNames[KK_COUNT] = {
     "poisson_begin", "layout", "seq_sum", "bicg_p_fused", "bicg_s_fused", "refine_residual",
     "refine_update", "sor_sweep32", "jacobi_sweep32", "bicg_p32", "bicg_q32", "bicg_s32",
     "bicg_t32", "bicg_xr32", "adj_velocity_bc", "adj_project", "adj_faces", "adj_nut",
-    "adj_predict", "adj_alm", "mg_smooth", "mg_transfer", "mg_coarse", "mg_pcg"};
+    "adj_predict", "adj_alm", "mg_smooth", "mg_transfer", "mg_coarse", "mg_pcg",
+    "jacobi_sweep2"};
 
 }  // namespace
 
@@ -2132,6 +2133,7 @@ int dalm_get_kernel_timing(dalm_handle *h, int index, const char **name, int64_t
         case KK_SOR_SWEEP: s = 2 * n; break;
         case KK_RESIDUAL_NORM: s = (h->pcfg.method == PM_JACOBI ? 3 : 2) * n; break;
         case KK_JACOBI_SWEEP: s = 3 * n; break;
+        case KK_JACOBI_SWEEP2: s = 3 * n; break;  // R x, rhs; W out: the pair's bytes
         case KK_BICG_INIT: s = 5 * n; break;
         case KK_BICG_P: s = 5 * n; break;
         case KK_BICG_Q: s = 3 * n; break;

@@ -389,6 +389,165 @@ k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
     }
 }
 
+// Two Jacobi sweeps in one pass over HBM (FP64): out = J(J(x)), J the
+// sweep of k_stencil<SK_JACOBI> with right-hand side rhs.  A block marches
+// its column segment through i; per plane it computes the first sweep on
+// the tile and a one-cell ring around it (34 x 10 cells, from x staged by
+// TMA in the wide box, 40 x 14, and rhs in the halo box, 36 x 10) into a
+// four-plane shared ring, and the second sweep on the tile one plane
+// behind.  The ring cells of the first sweep are recomputed by each block
+// that needs them (the unfused pair writes and re-reads the whole
+// intermediate vector instead): 3 vectors per cell instead of 6.  The
+// intermediate is zero outside the interior, as the unfused pair's scratch
+// vector is (its guide cells are never written), and every cell value comes
+// from the same diag / apply_a / relax as k_stencil's, so the result is the
+// unfused pair's bit for bit, in both arithmetic variants.
+//
+// Load L (0 <= L < nplanes + 4) brings x plane i0 - 2 + L and, for
+// 1 <= L <= nplanes + 2, rhs plane i0 - 2 + L into stage L % J2_STAGES.
+// First sweep at plane i0 - 1 + a reads x loads a .. a + 2 and rhs load
+// a + 1; the second sweep at plane i0 + b reads first-sweep planes b .. b + 2
+// and rhs load b + 2.  Iteration a computes first-sweep plane a, then (one
+// barrier later) second-sweep plane a - 2, and refills the stage of load
+// a - 1, whose last reader ran before that barrier.
+constexpr int J2_STAGES = 6;
+constexpr int J2_WK = TK + 2 * WIDE_HK, J2_WJ = TJ + 2 * WIDE_HJ;  // x box: 40 x 14
+constexpr int J2_HK = 2, J2_HKW = TK + 2 * J2_HK, J2_HJW = TJ + 2;  // rhs / ring: 36 x 10
+constexpr int J2_XB = J2_WK * J2_WJ * 8, J2_RB = J2_HKW * J2_HJW * 8;
+constexpr int J2_RBP = ((J2_RB + 127) / 128) * 128;  // stages stay 128-byte aligned
+constexpr int J2_STAGE = J2_XB + J2_RBP;
+constexpr int J2_RING = 2 * (TK + 2) + 2 * TJ;  // 84 cells around the tile
+constexpr int J2_SMEM = J2_STAGES * J2_STAGE + 4 * J2_RB;
+static_assert(J2_XB % 128 == 0 && J2_STAGE % 128 == 0, "TMA destinations 128-byte aligned");
+static_assert(J2_RING <= TILE_THREADS, "one ring cell per thread at most");
+
+// the q-th ring cell (0 <= q < 84) relative to the tile origin: rows -1 and
+// 8 over columns -1 .. 32, then columns -1 and 32 of rows 0 .. 7
+__device__ __forceinline__ void j2_ring_cell(int q, int &jj, int &kk) {
+    if (q < 2 * (TK + 2)) {
+        jj = q < TK + 2 ? -1 : TJ;
+        kk = (q < TK + 2 ? q : q - (TK + 2)) - 1;
+    } else {
+        const int t = q - 2 * (TK + 2);
+        jj = t >> 1;
+        kk = (t & 1) ? TK : -1;
+    }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(TILE_THREADS)
+k_jacobi2(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m_x,
+          const __grid_constant__ CUtensorMap m_rhs, double *out, KrylovState *st) {
+    using T = double;
+    if (st->done) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long bar[J2_STAGES];
+    const int u = blockIdx.x;
+    int i0, i1, j, k;
+    const bool active = S.column(u, i0, i1, j, k);
+    const int col = u % S.ncol;
+    const int k0 = S.box.lo[2] + (col % S.ntk) * TK, j0 = S.box.lo[1] + (col / S.ntk) * TJ;
+    const int nplanes = i1 - i0, nload = nplanes + 4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gc = g.gc;
+    T *ring = (T *)(smem + J2_STAGES * J2_STAGE);  // four first-sweep planes, 36 x 10 each
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < J2_STAGES; s++) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    auto issue = [&](int L) {
+        const int s = L % J2_STAGES;
+        unsigned char *base = smem + s * J2_STAGE;
+        const bool rhs = L >= 1 && L <= nplanes + 2;
+        mbar_expect_tx(&bar[s], J2_XB + (rhs ? J2_RB : 0));
+        tma_load_3d(base, &m_x, k0 - WIDE_HK + (int)g.off, j0 - WIDE_HJ, i0 - 2 + L, &bar[s]);
+        if (rhs)
+            tma_load_3d(base + J2_XB, &m_rhs, k0 - J2_HK + (int)g.off, j0 - 1, i0 - 2 + L, &bar[s]);
+    };
+    int issued = 0;
+    if (threadIdx.x == 0)
+        for (; issued < J2_STAGES && issued < nload; issued++) issue(issued);
+
+    // this thread's cells of the first sweep: the tile cell and at most one
+    // ring cell, relative to (j0, k0)
+    int rj = 0, rk = 0;
+    const bool has_ring = threadIdx.x < J2_RING;
+    if (has_ring) j2_ring_cell(threadIdx.x, rj, rk);
+    auto interior_jk = [&](int jj, int kk) {
+        const int jg = j0 + jj, kg = k0 + kk;
+        return jg >= gc && jg < g.ny - gc && kg >= gc && kg < g.nz - gc;
+    };
+    const bool tile_in = interior_jk(warp, lane), ring_in = has_ring && interior_jk(rj, rk);
+    ColumnCoef<T> cc{}, cr{};
+    if (tile_in) cc = column_coef<T>(C, j0 + warp, k0 + lane);
+    if (ring_in) cr = column_coef<T>(C, j0 + rj, k0 + rk);
+    const int sx = (int)g.sx;
+    const int cbase = active ? (int)g.at(i0, j, k) : 0;
+
+    // one cell of a sweep at plane ip: x values from the planes W, Cp, E at
+    // index xi (row stride rs), rhs at rhs[ri]
+    auto sweep = [&](int ip, const ColumnCoef<T> &c, const T *W, const T *Cp, const T *E, int xi,
+                     int rs, const T *rh, int ri) {
+        const T ac = diag<EXACT, T>((T)C.xpart[ip], c, C);
+        const T xc = Cp[xi];
+        const T ax = apply_a<EXACT, T>(ac, (T)C.ae[ip], (T)C.aw[ip], c, xc, E[xi], W[xi], Cp[xi + rs],
+                                       Cp[xi - rs], Cp[xi + 1], Cp[xi - 1]);
+        return xc + relax<EXACT, T>(rh[ri], ax, ac);
+    };
+    auto xplane = [&](int L) { return (const T *)(smem + (L % J2_STAGES) * J2_STAGE); };
+    auto rplane = [&](int L) { return (const T *)(smem + (L % J2_STAGES) * J2_STAGE + J2_XB); };
+    auto xidx = [](int jj, int kk) { return (jj + WIDE_HJ) * J2_WK + kk + WIDE_HK; };
+    auto hidx = [](int jj, int kk) { return (jj + 1) * J2_HKW + kk + J2_HK; };
+
+    int waited = 0;
+    bool fail = false;
+    for (int a = 0; a < nplanes + 2; a++) {
+        while (!fail && waited <= a + 2) {
+            fail = !mbar_wait(&bar[waited % J2_STAGES], (unsigned)((waited / J2_STAGES) & 1));
+            if (!fail) waited++;
+        }
+        if (!fail) {
+            // first sweep at plane i0 - 1 + a into ring slot a % 4
+            const int ip = i0 - 1 + a;
+            const bool plane_in = ip >= gc && ip < g.nx - gc;
+            T *R = ring + (a & 3) * (J2_HKW * J2_HJW);
+            const T *W = xplane(a), *Cp = xplane(a + 1), *E = xplane(a + 2), *rh = rplane(a + 1);
+            R[hidx(warp, lane)] = (plane_in && tile_in)
+                                      ? sweep(ip, cc, W, Cp, E, xidx(warp, lane), J2_WK, rh, hidx(warp, lane))
+                                      : (T)0;
+            if (has_ring)
+                R[hidx(rj, rk)] = (plane_in && ring_in)
+                                      ? sweep(ip, cr, W, Cp, E, xidx(rj, rk), J2_WK, rh, hidx(rj, rk))
+                                      : (T)0;
+        }
+        if (__syncthreads_or(fail)) break;
+        if (a >= 2 && active) {
+            // second sweep at plane i0 + b, b = a - 2
+            const int b = a - 2, ip = i0 + b;
+            const T *Aw = ring + (b & 3) * (J2_HKW * J2_HJW);
+            const T *Ac = ring + ((b + 1) & 3) * (J2_HKW * J2_HJW);
+            const T *Ae = ring + ((b + 2) & 3) * (J2_HKW * J2_HJW);
+            out[cbase + b * sx] = sweep(ip, cc, Aw, Ac, Ae, hidx(warp, lane), J2_HKW, rplane(b + 2),
+                                        hidx(warp, lane));
+        }
+        if (threadIdx.x == 0 && a >= 1 && issued < nload) {
+            fence_proxy_async();  // the released stage was read through the generic proxy
+            issue(issued++);
+        }
+    }
+    if (__syncthreads_or(fail)) {
+        // a bounded wait ran out: report, drain what is still in flight, stop
+        if (threadIdx.x == 0) {
+            st->wait_error = 1;
+            st->done = 1;
+            for (int L = waited; L < issued; L++)
+                mbar_wait(&bar[L % J2_STAGES], (unsigned)((L / J2_STAGES) & 1));
+        }
+    }
+}
+
 Box interior_box(const Grid &g) {
     return Box{{g.gc, g.gc, g.gc}, {g.nx - g.gc, g.ny - g.gc, g.nz - g.gc}};
 }
@@ -441,6 +600,20 @@ T *precondition(const LaunchCtx &L, const Grid &g, const PoissonCoef &C, const P
             for (int color = 0; color < 2; color++)
                 sor_sweep<T>(L, g, C, cfg, x, rhs, cfg.pc_relax, color, st);
         return x;
+    }
+    if constexpr (kF64<T>) {
+        if (cfg.pc_sweeps == 3) {  // the last two sweeps in one pass: M^-1 rhs into tmp
+            const Segments &S = cfg.seg;
+            const CUtensorMap &mx = cfg.maps->of(x).wide, &mr = cfg.maps->of(rhs).halo;
+            L.pre(KK_JACOBI_SWEEP2);
+            with_exact<T>(cfg.reference_sums != 0, [&](auto ex) {
+                auto kern = k_jacobi2<decltype(ex)::value>;
+                DALM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, J2_SMEM));
+                kern<<<S.count, TILE_THREADS, J2_SMEM, L.s>>>(g, C, S, mx, mr, tmp, st);
+            });
+            L.post(KK_JACOBI_SWEEP2);
+            return tmp;
+        }
     }
     T *cur = x, *nxt = tmp;
     for (int n = 1; n < cfg.pc_sweeps; n++) {
