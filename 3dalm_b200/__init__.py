@@ -57,7 +57,7 @@ class Options(C.Structure):
                 ("poisson_batch", C.c_int), ("use_graphs", C.c_int), ("profile", C.c_int),
                 ("reference_sums", C.c_int), ("fused_krylov", C.c_int),
                 ("refine_inner_it", C.c_int), ("write_output", C.c_int),
-                ("mixed_inner", C.c_int), ("reserved", C.c_int * 3)]
+                ("mixed_inner", C.c_int), ("fused_jacobi", C.c_int), ("reserved", C.c_int * 2)]
 
 
 _PD = C.POINTER(C.c_double)
@@ -100,7 +100,7 @@ class Solver:
                  time_average: bool = True, profile: bool = False, poisson_batch: int = 0,
                  limiter: int = MINMOD, reference_sums: bool = False, fused_krylov: bool = False,
                  refine_inner_it: int = 0, write_output: bool = False,
-                 mixed_inner: int = INNER_MULTIGRID):
+                 mixed_inner: int = INNER_MULTIGRID, fused_jacobi: bool = False):
         self.lib = load_library()
         self.h = C.c_void_p()
         self.opt = Options()
@@ -116,6 +116,7 @@ class Solver:
         self.opt.refine_inner_it = int(refine_inner_it)
         self.opt.write_output = int(write_output)
         self.opt.mixed_inner = int(mixed_inner)
+        self.opt.fused_jacobi = int(fused_jacobi)
         if case_dir is not None:
             self.initialize(case_dir)
 

@@ -353,6 +353,7 @@ struct dalm_handle {
         pcfg.pc_relax = cs.pc_relax;
         pcfg.pc_sweeps = (int)cs.pc_max_it;
         pcfg.reference_sums = opt.reference_sums ? 1 : 0;
+        pcfg.jacobi2 = opt.fused_jacobi ? 1 : 0;
         pcfg.seg = poisson_segments(g, sm_count);
         fused = opt.fused_krylov && fused_bicg_available(pcfg);
         // FP32 inner solves exist for BiCGStab only; SOR and Jacobi solves

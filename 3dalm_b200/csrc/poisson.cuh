@@ -65,6 +65,7 @@ struct PoissonConfig {
     double relax, pc_relax;
     int pc_sweeps;
     int reference_sums;  // 1: global sums in the reference's serial order
+    int jacobi2;         // 1: FP64 Jacobi(3): the last two sweeps in one pass
     Segments seg;        // column segments of the interior (one per block)
     const MapTable *maps;
 };

@@ -451,10 +451,19 @@ k_jacobi2(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gc = g.gc;
     T *ring = (T *)(smem + J2_STAGES * J2_STAGE);  // four first-sweep planes, 36 x 10 each
+    // per-plane coefficients of planes i0 - 1 .. i1 (index a = plane - i0 + 1)
+    __shared__ T s_xp[MAXCHUNK + 2], s_ae[MAXCHUNK + 2], s_aw[MAXCHUNK + 2];
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < J2_STAGES; s++) mbar_init(&bar[s], 1);
         fence_barrier_init();
+    }
+    if (threadIdx.x < nplanes + 2) {
+        const int ip = i0 - 1 + threadIdx.x;
+        const bool in = ip >= gc && ip < g.nx - gc;
+        s_xp[threadIdx.x] = in ? (T)C.xpart[ip] : (T)0;
+        s_ae[threadIdx.x] = in ? (T)C.ae[ip] : (T)0;
+        s_aw[threadIdx.x] = in ? (T)C.aw[ip] : (T)0;
     }
     __syncthreads();
     auto issue = [&](int L) {
@@ -486,16 +495,18 @@ k_jacobi2(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
     const int sx = (int)g.sx;
     const int cbase = active ? (int)g.at(i0, j, k) : 0;
 
-    // one cell of a sweep at plane ip: x values from the planes W, Cp, E at
-    // index xi (row stride rs), rhs at rhs[ri]
-    auto sweep = [&](int ip, const ColumnCoef<T> &c, const T *W, const T *Cp, const T *E, int xi,
-                     int rs, const T *rh, int ri) {
-        const T ac = diag<EXACT, T>((T)C.xpart[ip], c, C);
+    // one cell of a sweep at plane index a (plane i0 - 1 + a) with diagonal
+    // ac: x values from the planes W, Cp, E at index xi (row stride rs), rhs
+    // at rh[ri]; relax<EXACT>'s arithmetic, with 1/ac (fast variant) given
+    auto sweep = [&](int a, T ac, T rac, const ColumnCoef<T> &c, const T *W, const T *Cp,
+                     const T *E, int xi, int rs, const T *rh, int ri) {
         const T xc = Cp[xi];
-        const T ax = apply_a<EXACT, T>(ac, (T)C.ae[ip], (T)C.aw[ip], c, xc, E[xi], W[xi], Cp[xi + rs],
+        const T ax = apply_a<EXACT, T>(ac, s_ae[a], s_aw[a], c, xc, E[xi], W[xi], Cp[xi + rs],
                                        Cp[xi - rs], Cp[xi + 1], Cp[xi - 1]);
-        return xc + relax<EXACT, T>(rh[ri], ax, ac);
+        return xc + (EXACT ? relax<true, T>(rh[ri], ax, ac) : (rh[ri] - ax) * rac);
     };
+    auto inv = [](T ac) { return EXACT ? (T)0 : fast_rcp(ac); };
+    T ac_prev = 0, rac_prev = 0;  // the tile cell's diagonal at the previous iteration's plane
     auto xplane = [&](int L) { return (const T *)(smem + (L % J2_STAGES) * J2_STAGE); };
     auto rplane = [&](int L) { return (const T *)(smem + (L % J2_STAGES) * J2_STAGE + J2_XB); };
     auto xidx = [](int jj, int kk) { return (jj + WIDE_HJ) * J2_WK + kk + WIDE_HK; };
@@ -508,6 +519,9 @@ k_jacobi2(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
             fail = !mbar_wait(&bar[waited % J2_STAGES], (unsigned)((waited / J2_STAGES) & 1));
             if (!fail) waited++;
         }
+        // the tile cell's diagonal at first-sweep plane a (the second sweep
+        // reaches this plane in the next iteration)
+        const T ac = diag<EXACT, T>(s_xp[a], cc, C), rac = inv(ac);
         if (!fail) {
             // first sweep at plane i0 - 1 + a into ring slot a % 4
             const int ip = i0 - 1 + a;
@@ -515,23 +529,30 @@ k_jacobi2(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
             T *R = ring + (a & 3) * (J2_HKW * J2_HJW);
             const T *W = xplane(a), *Cp = xplane(a + 1), *E = xplane(a + 2), *rh = rplane(a + 1);
             R[hidx(warp, lane)] = (plane_in && tile_in)
-                                      ? sweep(ip, cc, W, Cp, E, xidx(warp, lane), J2_WK, rh, hidx(warp, lane))
+                                      ? sweep(a, ac, rac, cc, W, Cp, E, xidx(warp, lane), J2_WK, rh,
+                                              hidx(warp, lane))
                                       : (T)0;
-            if (has_ring)
-                R[hidx(rj, rk)] = (plane_in && ring_in)
-                                      ? sweep(ip, cr, W, Cp, E, xidx(rj, rk), J2_WK, rh, hidx(rj, rk))
-                                      : (T)0;
+            if (has_ring) {
+                T v = (T)0;
+                if (plane_in && ring_in) {
+                    const T acr = diag<EXACT, T>(s_xp[a], cr, C);
+                    v = sweep(a, acr, inv(acr), cr, W, Cp, E, xidx(rj, rk), J2_WK, rh, hidx(rj, rk));
+                }
+                R[hidx(rj, rk)] = v;
+            }
         }
         if (__syncthreads_or(fail)) break;
         if (a >= 2 && active) {
-            // second sweep at plane i0 + b, b = a - 2
-            const int b = a - 2, ip = i0 + b;
+            // second sweep at plane i0 + b, b = a - 2 (first-sweep plane index b + 1)
+            const int b = a - 2;
             const T *Aw = ring + (b & 3) * (J2_HKW * J2_HJW);
             const T *Ac = ring + ((b + 1) & 3) * (J2_HKW * J2_HJW);
             const T *Ae = ring + ((b + 2) & 3) * (J2_HKW * J2_HJW);
-            out[cbase + b * sx] = sweep(ip, cc, Aw, Ac, Ae, hidx(warp, lane), J2_HKW, rplane(b + 2),
-                                        hidx(warp, lane));
+            out[cbase + b * sx] = sweep(b + 1, ac_prev, rac_prev, cc, Aw, Ac, Ae, hidx(warp, lane),
+                                        J2_HKW, rplane(b + 2), hidx(warp, lane));
         }
+        ac_prev = ac;
+        rac_prev = rac;
         if (threadIdx.x == 0 && a >= 1 && issued < nload) {
             fence_proxy_async();  // the released stage was read through the generic proxy
             issue(issued++);
@@ -602,7 +623,7 @@ T *precondition(const LaunchCtx &L, const Grid &g, const PoissonCoef &C, const P
         return x;
     }
     if constexpr (kF64<T>) {
-        if (cfg.pc_sweeps == 3) {  // the last two sweeps in one pass: M^-1 rhs into tmp
+        if (cfg.jacobi2 && cfg.pc_sweeps == 3) {  // the last two sweeps in one pass: M^-1 rhs into tmp
             const Segments &S = cfg.seg;
             const CUtensorMap &mx = cfg.maps->of(x).wide, &mr = cfg.maps->of(rhs).halo;
             L.pre(KK_JACOBI_SWEEP2);

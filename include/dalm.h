@@ -151,7 +151,13 @@ typedef struct {
                              and a per-turbine turbines.csv every step   */
     int mixed_inner;      /* DALM_MIXED: the FP32 inner solver of each
                              refinement pass, enum dalm_mixed_inner      */
-    int reserved[3];
+    int fused_jacobi;     /* 1: the FP64 Jacobi(3) preconditioner's last
+                             two sweeps in one pass over HBM (3 instead of
+                             6 vectors per cell; same results bit for
+                             bit); 0 (default): one kernel per sweep,
+                             which is as fast under the power cap (the
+                             fused pair is instruction-bound)            */
+    int reserved[2];
 } dalm_options;
 
 /* Fills *opt with the defaults (FP64, minmod, device 0, time average on,

@@ -40,6 +40,7 @@ def test_default_options(lib):
     o = pkg.Options()
     lib.dalm_default_options(C.byref(o))
     assert (o.precision, o.limiter, o.device, o.time_average) == (pkg.FP64, pkg.MINMOD, 0, 1)
+    assert (o.fused_krylov, o.fused_jacobi) == (0, 0)
 
 
 def test_null_arguments_are_rejected(lib):

@@ -164,3 +164,35 @@ def test_c2_geometry_turbine_stage_by_stage(make_case):
     assert_steps_identical(a, b, "C2 geometry step 2")
     s.finalize()
     o.close()
+
+
+@pytest.mark.parametrize("reference_sums", [False, True], ids=["fast", "reference-order"])
+@pytest.mark.parametrize("name,over", [("tiny-bicg", {"n": MULTI_TILE, "dt": MULTI_TILE_DT}),
+                                       ("tiny-turbine", {})], ids=["multi-tile", "turbine"])
+def test_fused_jacobi_pair_bit_identical(make_case, name, over, reference_sums):
+    """opt.fused_jacobi: the Jacobi(3) preconditioner's last two sweeps in
+    one kernel (k_jacobi2, the intermediate sweep recomputed on a ring of
+    halo cells in shared memory) give the unfused pair's results bit for
+    bit, in both arithmetic variants, over five steps, iteration counts
+    included."""
+    pkg = package()
+    spec, mesh, d, U0, prof = make_case(name, **over)
+    runs = []
+    for fused in (False, True):
+        s = pkg.Solver(d, reference_sums=reference_sums, fused_jacobi=fused, profile=True)
+        if prof is not None:
+            s.set_inflow_profile(prof)
+        s.set_state(U0)
+        its = []
+        for _ in range(6):
+            s.step(1)
+            its.append(s.stats()["it"])
+        kt = s.kernel_timings()
+        runs.append((its, s.field("U"), s.field("p"), kt["jacobi_sweep2"]["launches"],
+                     kt["jacobi_sweep"]["launches"]))
+        s.finalize()
+    (its0, U0_, p0, j2_0, j1_0), (its1, U1, p1, j2_1, j1_1) = runs
+    assert j2_0 == 0 and j1_0 > 0 and j2_1 > 0 and j1_1 == 0, (j2_0, j1_0, j2_1, j1_1)
+    assert its0 == its1
+    np.testing.assert_array_equal(U1, U0_)
+    np.testing.assert_array_equal(p1, p0)
