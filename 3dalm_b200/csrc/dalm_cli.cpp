@@ -1,5 +1,6 @@
 // Command-line driver:
 //   dalm <case_dir> [--steps N] [--quiet] [--no-output] [--reference-sums] [--mixed]
+//        [--fused-jacobi]
 // Mirrors the reference's `solver <case_dir>` (src/solver.cpp:6-47): runs
 // steps 0..max_step (or N steps), prints the per-step line
 // `step time it err avg_div max_cfl` (src/solver.h:1188-1190), writes the
@@ -32,7 +33,7 @@ int main(int argc, char **argv) {
     if (argc < 2) {
         fprintf(stderr,
                 "usage: %s <case_dir> [--steps N] [--quiet] [--no-output] [--reference-sums] "
-                "[--mixed]\n",
+                "[--mixed] [--fused-jacobi]\n",
                 argv[0]);
         return 2;
     }
@@ -48,6 +49,7 @@ int main(int argc, char **argv) {
         else if (!strcmp(argv[a], "--no-output")) opt.write_output = 0;
         else if (!strcmp(argv[a], "--reference-sums")) opt.reference_sums = 1;
         else if (!strcmp(argv[a], "--mixed")) opt.precision = DALM_MIXED;
+        else if (!strcmp(argv[a], "--fused-jacobi")) opt.fused_jacobi = 1;
         else {
             fprintf(stderr, "unknown option %s\n", argv[a]);
             return 2;
