@@ -197,7 +197,11 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms.  start()
+    returns once the first sample has arrived (at most 3 s), and stop() waits
+    (at most 0.6 s) for one sample after the timed region, so that a region
+    shorter than the sampling interval is still covered: the summary takes the
+    last sample before the region and every one from it to the first after."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -218,6 +222,11 @@ class ClockSampler:
             self.thread.start()
         except OSError:
             self.proc = None
+            return
+        t = time.perf_counter()
+        while not self.lines and time.perf_counter() - t < 3.0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.first = max(0, len(self.lines) - 1)  # the last sample before the region
 
     def _read(self):
         for line in self.proc.stdout:
@@ -226,6 +235,9 @@ class ClockSampler:
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        n, t = len(self.lines), time.perf_counter()
+        while len(self.lines) == n and time.perf_counter() - t < 0.6 and self.proc.poll() is None:
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -234,7 +246,7 @@ class ClockSampler:
         self.thread.join(timeout=2)
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[getattr(self, "first", 0):]:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
