@@ -18,7 +18,7 @@
 // cells of a column and marches through a chunk of i-planes.  The stencil
 // kernels stage each plane of their operand (one-cell halo in j, 16 bytes of
 // halo in k) and of their point-wise input in shared memory with TMA
-// (cp.async.bulk.tensor), NSTAGE planes deep, and compute two planes per
+// (cp.async.bulk.tensor), NSTAGE planes deep, and compute PPP planes per
 // pass, so the loads of the next planes are in flight while the current
 // ones are computed.
 #include <cfloat>
@@ -214,7 +214,8 @@ k_refine_update(Grid g, Segments S, double *x, const float *e, double sign) {
 
 // ------------------------------------------------------- TMA stencil sweeps
 
-constexpr int NSTAGE = 8;
+constexpr int NSTAGE = 8;  // TMA ring depth (planes)
+constexpr int PPP = 2;     // planes computed per pass (one block barrier each)
 constexpr int MAXCHUNK = 32;  // Segments caps a chunk at 32 planes
 
 // shared-memory geometry of one ring stage for element type T
@@ -253,7 +254,7 @@ struct StencilArgs {
 // plane i0 - 1 + L of the operand (halo box) and, for the planes the block
 // computes, of the point-wise input (plain box) into ring stage L % NSTAGE.
 // Plane i0 + n is computed from loads n, n + 1, n + 2.  Each pass computes
-// two planes and then refills the two stages it released.
+// PPP planes and then refills the PPP stages it released.
 template <int KIND, bool EXACT, typename T>
 __global__ void __launch_bounds__(TILE_THREADS)
 k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap m_op,
@@ -352,15 +353,16 @@ k_stencil(Grid g, PoissonCoef C, Segments S, const __grid_constant__ CUtensorMap
 
     int waited = 0;
     bool fail = false;
-    for (int n = 0; n < nplanes; n += 2) {
-        const int m = nplanes - n < 2 ? nplanes - n : 2;
+    for (int n = 0; n < nplanes; n += PPP) {
+        const int m = nplanes - n < PPP ? nplanes - n : PPP;
         while (!fail && waited <= n + m + 1) {
             fail = !mbar_wait(&bar[waited % NSTAGE], (unsigned)((waited / NSTAGE) & 1));
             if (!fail) waited++;
         }
         if (!fail && active) {
-            cell(n);
-            if (m == 2) cell(n + 1);
+#pragma unroll
+            for (int q = 0; q < PPP; q++)
+                if (q < m) cell(n + q);
         }
         if (__syncthreads_or(fail)) break;
         if (threadIdx.x == 0) {
@@ -589,8 +591,10 @@ void stencil_launch(const LaunchCtx &L, int kind_tag, const Grid &g, const Poiss
     const size_t smem = (size_t)NSTAGE * Geo<T>::STAGE;
     L.pre(kind_tag);
     with_exact<T>(cfg.reference_sums != 0, [&](auto ex) {
-        k_stencil<KIND, decltype(ex)::value, T>
-            <<<S.count, TILE_THREADS, smem, L.s>>>(g, C, S, mo, mp, A, part, st);
+        auto kern = k_stencil<KIND, decltype(ex)::value, T>;
+        if (smem > 48 * 1024)
+            DALM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<S.count, TILE_THREADS, smem, L.s>>>(g, C, S, mo, mp, A, part, st);
     });
     L.post(kind_tag);
 }
