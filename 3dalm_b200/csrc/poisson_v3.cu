@@ -215,7 +215,9 @@ k_refine_update(Grid g, Segments S, double *x, const float *e, double sign) {
 // ------------------------------------------------------- TMA stencil sweeps
 
 constexpr int NSTAGE = 8;  // TMA ring depth (planes)
-constexpr int PPP = 2;     // planes computed per pass (one block barrier each)
+constexpr int PPP = 3;     // planes computed per pass (one block barrier each);
+                           // 3 measured ~1 % faster over the C4 step than 2, and
+                           // 4 with a 10-stage ring slower (3 blocks per SM)
 constexpr int MAXCHUNK = 32;  // Segments caps a chunk at 32 planes
 
 // shared-memory geometry of one ring stage for element type T
